@@ -1,0 +1,345 @@
+/*
+ * msb200.h - C-ABI of the B200 capsule contact-mechanics backend.
+ *
+ * Every entry point takes plain pointers, sizes and POD structs and returns an
+ * int status (MSB_OK = 0).  Nothing here mentions a C++ or torch type, so the
+ * engine's C++ ComputeBackend, a Python ctypes binding or any other FFI can
+ * bind it directly.  Each function names the reference interface it replaces
+ * (paths are relative to the MicroSimulator source tree).
+ *
+ * Error mapping (reference exceptions -> status):
+ *   std::invalid_argument -> MSB_ERR_INVALID_ARGUMENT
+ *   std::overflow_error   -> MSB_ERR_OVERFLOW
+ *   std::runtime_error    -> MSB_ERR_RUNTIME   (e.g. a step that cannot
+ *                            resolve its contacts, cpp/core/contact_dynamics.cpp:745-748)
+ *   CUDA errors           -> MSB_ERR_CUDA      (cpp/cuda/cuda_backend.cu:33-37 throws
+ *                            std::runtime_error with the CUDA text)
+ * msb_last_error() returns the message of the last failure on a context.
+ * Solver non-convergence is not an error: it is msb_contact_solve_report.status,
+ * as ContactSolveReport.status is (cpp/include/microsimulator/contact_dynamics.hpp:244-255).
+ */
+#ifndef MSB200_H
+#define MSB200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+enum msb_status {
+  MSB_OK = 0,
+  MSB_ERR_INVALID_ARGUMENT = 1,
+  MSB_ERR_OVERFLOW = 2,
+  MSB_ERR_RUNTIME = 3,
+  MSB_ERR_CUDA = 4,
+  /* The output array was too small; *count holds the size that is needed and
+   * nothing was written.  Call again with a larger array. */
+  MSB_ERR_CAPACITY = 5,
+  /* A device-side check failed (index out of range, iteration cap of a
+   * device loop); the kernel skipped the access and reported it. */
+  MSB_ERR_DEVICE_CHECK = 6,
+  MSB_ERR_NO_DEVICE = 7
+};
+
+/* Solver outcome, ContactSolveStatus (contact_dynamics.hpp:244-248). */
+enum msb_solve_status {
+  MSB_SOLVE_CONVERGED = 0,
+  MSB_SOLVE_ITERATION_LIMIT = 1,
+  MSB_SOLVE_BREAKDOWN = 2
+};
+
+/* GrowthLoadLaw (contact_dynamics.hpp:151-159). */
+enum msb_growth_load_law {
+  MSB_GROWTH_LAW_NONE = 0,
+  MSB_GROWTH_LAW_EXPONENTIAL = 1,
+  MSB_GROWTH_LAW_LINEAR = 2
+};
+
+/* ExternalConstraintKind / ConstraintRegion / RodContactLocation
+ * (cpp/include/microsimulator/constraints.hpp:16-36). */
+enum msb_constraint_kind {
+  MSB_CONSTRAINT_PLANE = 0,
+  MSB_CONSTRAINT_SPHERE = 1,
+  MSB_CONSTRAINT_BOX = 2,
+  MSB_CONSTRAINT_CYLINDER = 3
+};
+enum msb_constraint_region { MSB_REGION_OUTSIDE = 0, MSB_REGION_INSIDE = 1 };
+enum msb_rod_location { MSB_ROD_NEGATIVE = 0, MSB_ROD_POSITIVE = 1, MSB_ROD_INTERIOR = 2 };
+
+/* ------------------------------------------------------------------- types */
+typedef struct msb_vec3 {
+  float x, y, z;
+} msb_vec3;
+
+/* The cells of a WorldState as structure-of-arrays views, by slot
+ * (CellGeometryView + CellAttributeView, world_state.hpp:58-78).  Positions,
+ * directions and lengths are written back by the stepping calls; the other
+ * arrays are only read.  `fixed` holds 0 or 1 per cell. */
+typedef struct msb_cell_arrays {
+  uint64_t count;
+  const uint64_t* ids;
+  float* position_x;
+  float* position_y;
+  float* position_z;
+  float* direction_x;
+  float* direction_y;
+  float* direction_z;
+  float* lengths;
+  const float* radii;
+  const float* growth_rates;
+  const uint8_t* fixed;
+} msb_cell_arrays;
+
+/* ContactParameters (contact_graph.hpp:13-17). */
+typedef struct msb_contact_parameters {
+  float activation_margin;
+  float parallel_sine_threshold;
+  float degeneracy_epsilon;
+} msb_contact_parameters;
+
+/* CellContact (contact_graph.hpp:19-29).  64 bytes. */
+typedef struct msb_cell_contact {
+  uint64_t first_id;
+  uint64_t second_id;
+  uint32_t first_slot;
+  uint32_t second_slot;
+  uint32_t ordinal;
+  msb_vec3 point_on_first;
+  msb_vec3 normal;
+  float signed_separation;
+  float weight;
+  uint32_t reserved;
+} msb_cell_contact;
+
+/* One constraint of a ConstraintSet (constraints.hpp:66-96), flattened.
+ *   plane:    a = point,  b = inward normal
+ *   sphere:   a = center, radius
+ *   box:      a = center, b = half extents
+ *   cylinder: a = center, radius, half_height (axis along z) */
+typedef struct msb_constraint {
+  uint64_t id;
+  uint32_t kind;           /* msb_constraint_kind */
+  uint32_t allowed_region; /* msb_constraint_region */
+  msb_vec3 a;
+  msb_vec3 b;
+  float radius;
+  float half_height;
+  float coefficient;
+  uint32_t reserved;
+} msb_constraint;
+
+/* ConstraintContactParameters (constraints.hpp:141-144). */
+typedef struct msb_constraint_contact_parameters {
+  float activation_margin;
+  float degeneracy_epsilon;
+} msb_constraint_contact_parameters;
+
+/* ExternalContact (constraints.hpp:146-156).  56 bytes. */
+typedef struct msb_external_contact {
+  uint64_t cell_id;
+  uint64_t constraint_id;
+  uint32_t cell_slot;
+  uint32_t constraint_kind; /* msb_constraint_kind */
+  uint32_t location;        /* msb_rod_location */
+  msb_vec3 point_on_cell;
+  msb_vec3 normal;
+  float signed_separation;
+  float weight;
+  uint32_t reserved;
+} msb_external_contact;
+
+/* GrowthLoadResponse (contact_dynamics.hpp:161-166). */
+typedef struct msb_growth_load_response {
+  uint32_t law; /* msb_growth_load_law */
+  float sensitivity;
+  float free_load;
+  float stall_load;
+} msb_growth_load_response;
+
+/* ContactRow (contact_dynamics.hpp:210-219).  72 bytes; a row against a
+ * constraint has second_slot = 0xFFFFFFFF (invalid_slot). */
+typedef struct msb_contact_row {
+  uint32_t first_slot;
+  uint32_t second_slot;
+  float first_jacobian[6];
+  float second_jacobian[6];
+  float first_length_lever;
+  float second_length_lever;
+  float offset;
+  float compliance;
+} msb_contact_row;
+
+/* ContactBody (contact_dynamics.hpp:224-231).  52 bytes. */
+typedef struct msb_contact_body {
+  msb_vec3 axis;
+  float translational_mobility;
+  float transverse_mobility;
+  float axial_mobility;
+  float length_rate;
+  float drift[6];
+} msb_contact_body;
+
+/* ContactSystem (contact_dynamics.hpp:237-242). */
+typedef struct msb_contact_system {
+  const msb_contact_row* rows;
+  uint64_t row_count;
+  const msb_contact_body* bodies;
+  uint64_t body_count;
+  float dt;
+  msb_growth_load_response growth;
+} msb_contact_system;
+
+/* ContactSolveParameters / ContactSolveReport (contact_dynamics.hpp:250-260). */
+typedef struct msb_contact_solve_parameters {
+  float tolerance;
+  uint32_t max_iterations;
+} msb_contact_solve_parameters;
+
+typedef struct msb_contact_solve_report {
+  uint32_t status; /* msb_solve_status */
+  uint32_t iterations;
+  float residual;
+} msb_contact_solve_report;
+
+/* ContactDynamicsParameters (contact_dynamics.hpp:173-201). */
+typedef struct msb_contact_dynamics_parameters {
+  float drag;
+  float contact_stiffness;
+  float wall_stiffness;
+  float overlap_tolerance;
+  float candidate_margin;
+  float max_overlap_recovery;
+  float max_growth_fraction;
+  uint32_t max_iterations;
+  uint32_t max_refinements;
+  uint32_t max_step_halvings;
+  uint32_t flow_drift; /* must be 0: the flow-drift coupling is not part of this backend */
+  msb_growth_load_response growth;
+} msb_contact_dynamics_parameters;
+
+/* ContactDynamicsReport (contact_dynamics.hpp:291-299). */
+typedef struct msb_contact_dynamics_report {
+  uint32_t substeps;
+  uint32_t halvings;
+  uint32_t refinements;
+  uint32_t reserved;
+  uint64_t iterations;
+  uint64_t max_rows;
+  float max_overlap;
+  uint32_t reserved2;
+} msb_contact_dynamics_report;
+
+/* ContactDynamicsResult arrays (contact_dynamics.hpp:301-309), by slot.
+ * Any pointer may be NULL when the caller does not want that output.
+ * center_velocities holds x, y, z per cell (3 * count floats). */
+typedef struct msb_contact_dynamics_outputs {
+  float* center_velocities;
+  float* axial_loads;
+  float* length_increments;
+} msb_contact_dynamics_outputs;
+
+typedef struct msb_context msb_context;
+
+/* ---------------------------------------------------------- backend handle */
+
+/* cuda_backend_device_count() (cpp/include/microsimulator/backend.hpp:62). */
+size_t msb_device_count(void);
+
+/* make_cuda_backend(device_index) (backend.hpp:60; cpp/cuda/cuda_backend.cu:1529-1541).
+ * The context owns its device buffers (grown on demand) and one non-blocking
+ * stream.  Calls on one context must not overlap; separate contexts may run
+ * from separate threads. */
+int msb_context_create(uint32_t device_index, msb_context** out);
+void msb_context_destroy(msb_context* context);
+
+/* Text of the last failure on `context` (empty if none). */
+const char* msb_last_error(const msb_context* context);
+
+/* BackendInfo (types.hpp:88-94): the device name, e.g. "NVIDIA B200". */
+int msb_backend_info(const msb_context* context, char* device_name, size_t capacity);
+
+/* ------------------------------------------------------ contact detection */
+
+/* ComputeBackend::find_cell_contacts (backend.hpp:35-36), with the behaviour of
+ * find_cell_contacts_cpu (cpp/cpu/cpu_contacts.cpp:216-219): every capsule pair
+ * whose padded boxes overlap and whose signed separation is below the
+ * activation margin, one or two contacts per pair, sorted by
+ * (first_id, second_id, ordinal).  `cells` are host arrays.  Writes at most
+ * `capacity` contacts; *count receives the total. */
+int msb_find_cell_contacts(msb_context* context, const msb_cell_arrays* cells,
+                           const msb_contact_parameters* parameters, msb_cell_contact* contacts,
+                           uint64_t capacity, uint64_t* count);
+
+/* ComputeBackend::find_external_contacts (backend.hpp:37-39) when every_face is
+ * 0 (find_external_contacts_cpu, cpp/cpu/cpu_constraints.cpp:602-606), and
+ * find_external_contact_faces (constraints.hpp:190-192, cpu_constraints.cpp:608-612)
+ * when every_face is 1.  Sorted by (cell_id, constraint_id, location). */
+int msb_find_external_contacts(msb_context* context, const msb_cell_arrays* cells,
+                               const msb_constraint* constraints, uint64_t constraint_count,
+                               const msb_constraint_contact_parameters* parameters,
+                               uint32_t every_face, msb_external_contact* contacts,
+                               uint64_t capacity, uint64_t* count);
+
+/* --------------------------------------------------------- contact solve */
+
+/* ComputeBackend::solve_contact_forces (backend.hpp:41-43): Barzilai-Borwein
+ * projected gradient from `initial_multipliers` (cpp/core/contact_solver.hpp:86-120,
+ * cpp/cpu/cpu_contact_dynamics.cpp:262-338), run to convergence on the device.
+ * Host arrays; `multipliers` receives row_count values. */
+int msb_solve_contact_forces(msb_context* context, const msb_contact_system* system,
+                             const float* initial_multipliers,
+                             const msb_contact_solve_parameters* parameters, float* multipliers,
+                             msb_contact_solve_report* report);
+
+/* evaluate_contact_response (contact_dynamics.hpp:277-278): per body the
+ * velocity then angular velocity (6 floats), the axial load and the loaded
+ * elongation rate.  Any output may be NULL. */
+int msb_evaluate_contact_response(msb_context* context, const msb_contact_system* system,
+                                  const float* multipliers, float* velocities, float* loads,
+                                  float* length_rates);
+
+/* evaluate_contact_gaps (contact_dynamics.hpp:280-281). */
+int msb_evaluate_contact_gaps(msb_context* context, const msb_contact_system* system,
+                              const float* multipliers, float* gaps);
+
+/* contact_system_diagonal_bound (contact_dynamics.hpp:285). */
+int msb_contact_system_diagonal_bound(msb_context* context, const msb_contact_system* system,
+                                      float* bound);
+
+/* ------------------------------------------------------------ whole step */
+
+/* The contact-dynamics step of Simulation::step(dt, dynamics, contacts,
+ * constraints) (cpp/core/simulation.cpp:387-397): detail::advance_contact_dynamics
+ * (cpp/core/contact_stepper.hpp:32-35, cpp/core/contact_dynamics.cpp:676-782) with
+ * every per-cell, per-row and per-contact pass on the device and the substep
+ * controller on the host.  `cells` are host arrays; positions, directions and
+ * lengths are updated in place.  On failure the arrays are left unchanged. */
+int msb_advance_contact_dynamics(msb_context* context, msb_cell_arrays* cells,
+                                 const msb_constraint* constraints, uint64_t constraint_count,
+                                 float dt, const msb_contact_dynamics_parameters* dynamics,
+                                 const msb_contact_parameters* contacts,
+                                 const msb_constraint_contact_parameters* constraint_parameters,
+                                 msb_contact_dynamics_report* report,
+                                 msb_contact_dynamics_outputs* outputs);
+
+/* The same step with every array of `cells` and `outputs` in device memory of
+ * the context's GPU (for callers that keep the world resident in HBM). */
+int msb_advance_contact_dynamics_device(
+    msb_context* context, msb_cell_arrays* cells, const msb_constraint* constraints,
+    uint64_t constraint_count, float dt, const msb_contact_dynamics_parameters* dynamics,
+    const msb_contact_parameters* contacts,
+    const msb_constraint_contact_parameters* constraint_parameters,
+    msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs);
+
+/* Kernel launches issued by this context since it was created (for the
+ * launch counts that benchmarks report). */
+uint64_t msb_launch_count(const msb_context* context);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MSB200_H */
