@@ -1,0 +1,363 @@
+"""Throughput of the capsule contact-mechanics step: cell-steps/s.
+
+Workload (default): 1,000,000 capsules near jamming (area fraction 0.85,
+lengths log-normal mu = ln 3 um, sigma 0.2, radius 0.5 um, orientations
+uniform), open domain derived from N and the fraction, growth rate 0.5
+(+1 % length per step), 2 % of the cells divided per step with +-0.02 rad
+daughter turns, dt 0.02, overlap tolerance 5e-4 um (1e-3 radius).  A step is
+Simulation::step(dt, dynamics): the whole contact-dynamics step, relaxed to
+the tolerance.  Divisions are input preparation and run between steps.
+
+  value  steps on cells resident in HBM (device-pointer C-ABI call), timed
+         with CUDA events, max over ranks
+  e2e    the same steps through the host-buffer C-ABI call, host<->device
+         copies inside the timed region
+  roofline  the BB iteration (body pass + row pass) of the last solved
+         system, CUDA events on the backend's stream, against algorithmic
+         bytes R*96 + N*128 per iteration
+  cpu_baseline  the reference CPU backend (compiled from its sources) on a
+         bounded sample of the same workload, all host threads
+
+--impl reference prints the reference CPU backend's line on that sample.
+Multi-GPU: each rank steps its own independent colony (replicas; there is no
+data-path collective).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+DT = 0.02
+TOLERANCE = 5.0e-4
+DIVISION_FRACTION = 0.02
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cells", type=int, default=1_000_000)
+    p.add_argument("--cpu-cells", type=int, default=50_000)
+    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--seed", type=int, default=42)
+    p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
+    return p.parse_args()
+
+
+def dynamics():
+    from microsimulator_b200.types import ContactDynamicsParameters
+
+    return ContactDynamicsParameters(overlap_tolerance=TOLERANCE)
+
+
+def divide(world, step, seed):
+    from microsimulator_b200 import workloads
+
+    plan = workloads.plan_divisions(world, DIVISION_FRACTION, seed=seed * 100003 + step)
+    world.divide_many(plan.parents, 0.5, plan.rotations)
+    return plan
+
+
+class Clocks:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except FileNotFoundError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        self.file.flush()
+        rows = [line.split(",") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
+                          and "Not" not in r[5 + k]})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    path = ROOT / "MEASURED_PEAKS.json"
+    if path.exists():
+        peaks = json.loads(path.read_text())
+        return float(peaks["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """DRAM bytes per BB iteration per row and per body from the committed ncu
+    summary (profiles/bb_iteration_traffic.json), scaled to a launch by the
+    system's size; None without one."""
+    path = ROOT / "profiles" / "bb_iteration_traffic.json"
+    if not path.exists():
+        return None
+    return json.loads(path.read_text())
+
+
+def run_reference_sample(args, seconds, steps_cap):
+    """The reference CPU backend on a bounded sample of the workload."""
+    from microsimulator_b200 import workloads
+    from oracle.native import REFERENCE_PATH, Reference
+
+    if not REFERENCE_PATH.exists():
+        return None
+    ref = Reference()
+    world = workloads.jammed(n=args.cpu_cells, seed=args.seed)
+    handle = ref.world_create(world)
+    try:
+        plan_world = world.copy()
+        for step in range(2):  # the overlap of the random start resolves here
+            plan = divide(plan_world, step, args.seed)
+            ref.world_divide(handle, plan.parents, plan.rotations)
+            ref.world_step(handle, DT, dynamics())
+            ref.world_read(handle, plan_world)
+            plan_world.next_id = int(plan_world.ids.max()) + 1
+        cells_steps = 0
+        elapsed = 0.0
+        steps = 0
+        while steps < steps_cap and (elapsed < seconds or steps == 0):
+            plan = divide(plan_world, steps + 2, args.seed)
+            ref.world_divide(handle, plan.parents, plan.rotations)
+            t0 = time.perf_counter()
+            ref.world_step(handle, DT, dynamics())
+            elapsed += time.perf_counter() - t0
+            cells_steps += len(plan_world)
+            ref.world_read(handle, plan_world)
+            plan_world.next_id = int(plan_world.ids.max()) + 1
+            steps += 1
+        return {"value": cells_steps / elapsed, "unit": "cell-steps/s", "cores": ref.thread_count(),
+                "kind": "reference",
+                "sample": f"{args.cpu_cells} capsules of the same distribution and area fraction, "
+                          f"{steps} timed steps after 2 untimed, {elapsed:.1f} s"}
+    finally:
+        ref.world_destroy(handle)
+
+
+def config(args, world_size):
+    return {
+        "workload": f"jammed colony, {args.cells} capsules, area fraction 0.85, log-normal lengths, "
+                    "growth 0.5, 2% divisions/step, dt 0.02, tol 5e-4 um (1e-3 r)",
+        "cells_per_gpu": args.cells,
+        "parallelism": f"replicas{world_size}",
+        "l2": "inputs larger than L2 (working set > 126 MB at 1M capsules)",
+    }
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    sample = run_reference_sample(args, seconds=1e9, steps_cap=max(1, args.steps))
+    if sample is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmsref.so was not built"}))
+        return
+    print(json.dumps({
+        "impl": "reference",
+        "metric": "cell-steps/s at 1M capsules, 1e-3 overlap tol",
+        "value": sample["value"], "unit": "cell-steps/s", "n_gpus": world_size, "steps": args.steps,
+        "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic", "config": config(args, world_size),
+        "cpu_baseline": sample,
+        "e2e": {"value": sample["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }))
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+    import torch
+
+    from microsimulator_b200 import workloads
+    from microsimulator_b200.backend import B200Backend, DeviceCells
+
+    rank = int(os.environ.get("RANK", "0"))
+    world_size = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world_size > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    backend = B200Backend(local)
+    world = workloads.jammed(n=args.cells, seed=args.seed + rank)
+    dyn = dynamics()
+
+    def device_step(step):
+        divide(world, step, args.seed + rank)
+        cells = DeviceCells(world, device=f"cuda:{local}")
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        report = backend.advance_contact_dynamics_device(cells, None, DT, dyn)
+        end.record()
+        torch.cuda.synchronize()
+        cells.download(world)
+        world.next_id = int(world.ids.max()) + 1
+        return start.elapsed_time(end), report
+
+    for step in range(args.warmup):
+        device_step(step)
+    snapshot = world.copy()
+    barrier()
+    launches0 = backend.launch_count()
+    total_ms = 0.0
+    cell_steps = 0
+    iterations = 0
+    with Clocks(local) as clocks:
+        for k in range(args.steps):
+            n_before = len(world)
+            ms, report = device_step(args.warmup + k)
+            total_ms += ms
+            cell_steps += len(world)
+            iterations += report.iterations
+    barrier()
+    launches = backend.launch_count() - launches0
+    prof = backend.profile_iterations(20)
+
+    # e2e: the same steps from the same state through the host-buffer call.
+    e2e = None
+    if not args.no_e2e:
+        world = snapshot
+        e2e_s = 0.0
+        e2e_cells = 0
+        h2d = d2h = 0
+        for k in range(args.steps):
+            divide(world, args.warmup + k, args.seed + rank)
+            n = len(world)
+            barrier()
+            t0 = time.perf_counter()
+            backend.advance_contact_dynamics(world, None, DT, dyn)
+            torch.cuda.synchronize()
+            e2e_s += time.perf_counter() - t0
+            world.next_id = int(world.ids.max()) + 1
+            e2e_cells += n
+            h2d += n * (8 + 8 * 4 + 4 + 1)
+            d2h += n * (7 * 4 + 5 * 4)
+        e2e_total = e2e_s
+        if dist is not None:
+            t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e2e_total = float(t.item())
+        e2e = {"value": e2e_cells * world_size / e2e_total, "unit": "cell-steps/s",
+               "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
+
+    total = total_ms
+    if dist is not None:
+        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total = float(t.item())
+    value = cell_steps * world_size / (total * 1e-3)
+
+    rows, bodies = prof["rows"], prof["bodies"]
+    algorithmic = rows * 96 + bodies * 128
+    iteration_ms = prof["body_ms"] + prof["row_ms"]
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic / (iteration_ms * 1e-3) / 1e9
+    traffic = ncu_traffic()
+    traffic_bytes = None
+    if traffic is not None:
+        traffic_bytes = rows * traffic["bytes_per_row"] + bodies * traffic["bytes_per_body"]
+
+    cpu = None
+    if rank == 0 and world_size == 1 and not args.no_cpu:
+        cpu = run_reference_sample(args, seconds=args.cpu_seconds, steps_cap=50)
+
+    if rank == 0:
+        line = {
+            "metric": "cell-steps/s at 1M capsules, 1e-3 overlap tol",
+            "value": value,
+            "unit": "cell-steps/s",
+            "n_gpus": world_size,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": total / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f32",
+            "data": "synthetic",
+            "config": config(args, world_size),
+            "path": "plain",
+            "bb_iterations_per_step": iterations / args.steps,
+            "roofline": {
+                "kernel": "bb_iteration (body pass + row pass)",
+                "bound": "hbm",
+                "achieved": achieved,
+                "peak": peak,
+                "peak_kind": f"{peak_kind} hbm_gbs",
+                "unit": "GB/s",
+                "frac": achieved / peak,
+                "traffic": traffic_bytes,
+                "algorithmic_bytes": algorithmic,
+                "iteration_ms": iteration_ms,
+                "body_ms": prof["body_ms"],
+                "row_ms": prof["row_ms"],
+                "rows": rows,
+                "bodies": bodies,
+            },
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line))
+    backend.close()
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

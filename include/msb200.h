@@ -334,6 +334,13 @@ int msb_advance_contact_dynamics_device(
     const msb_constraint_contact_parameters* constraint_parameters,
     msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs);
 
+/* Measurement hook, no counterpart in the reference: runs `iterations` more
+ * projected iterations of the last system this context solved, timing each
+ * pass with CUDA events on the context's stream; returns the mean duration
+ * of the body pass and of the row pass and the system's rows and bodies. */
+int msb_profile_iterations(msb_context* context, uint32_t iterations, float* body_ms, float* row_ms,
+                           uint64_t* rows, uint64_t* bodies);
+
 /* Kernel launches issued by this context since it was created (for the
  * launch counts that benchmarks report). */
 uint64_t msb_launch_count(const msb_context* context);

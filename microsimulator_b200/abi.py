@@ -372,6 +372,10 @@ SIGNATURES = {
         ],
     ),
     "msb_launch_count": (c_uint64, [c_void_p]),
+    "msb_profile_iterations": (
+        c_int,
+        [c_void_p, c_uint32, POINTER(c_float), POINTER(c_float), POINTER(c_uint64), POINTER(c_uint64)],
+    ),
 }
 
 _library = None

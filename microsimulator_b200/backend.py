@@ -1,0 +1,269 @@
+"""The B200 contact backend behind the reference's ComputeBackend contact
+methods (cpp/include/microsimulator/backend.hpp:35-43), through the C-ABI of
+``include/msb200.h``.
+
+Every call runs on the GPU; there is no CPU path.  Errors come back as the
+exceptions the reference raises: ``ValueError`` for std::invalid_argument,
+``OverflowError`` for std::overflow_error, ``abi.NativeError`` (a
+RuntimeError) for std::runtime_error and CUDA failures.
+"""
+
+from __future__ import annotations
+
+import ctypes
+from ctypes import c_float, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+from . import abi
+from .types import (
+    ConstraintContactParameters,
+    ContactDynamicsParameters,
+    ContactDynamicsReport,
+    ContactDynamicsResult,
+    ContactParameters,
+    ContactResponse,
+    ContactSolveParameters,
+    ContactSolveReport,
+    ContactSolveResult,
+    ContactSystem,
+)
+
+
+def device_count() -> int:
+    """cuda_backend_device_count()."""
+    return int(abi.load_library().msb_device_count())
+
+
+class B200Backend:
+    """make_cuda_backend(device_index): one context, one stream, its buffers."""
+
+    def __init__(self, device_index: int = 0):
+        self._lib = abi.load_library()
+        handle = c_void_p()
+        status = self._lib.msb_context_create(device_index, ctypes.byref(handle))
+        if status != abi.OK:
+            raise abi.NativeError(status, f"could not create a B200 backend on device {device_index} (status {status})")
+        self._handle = handle
+        self.device_index = device_index
+        self._capacity = 1024
+
+    def close(self) -> None:
+        if getattr(self, "_handle", None):
+            self._lib.msb_context_destroy(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- helpers --------------------------------------------------------
+    def _check(self, status: int) -> None:
+        if status != abi.OK:
+            abi.raise_for_status(status, self._lib.msb_last_error(self._handle).decode())
+
+    def info(self) -> dict:
+        buffer = ctypes.create_string_buffer(256)
+        self._check(self._lib.msb_backend_info(self._handle, buffer, 256))
+        return {"kind": "cuda", "name": "B200 contact backend", "device": buffer.value.decode(),
+                "device_index": self.device_index, "native": True}
+
+    def launch_count(self) -> int:
+        return int(self._lib.msb_launch_count(self._handle))
+
+    def profile_iterations(self, iterations: int = 20) -> dict:
+        """Mean device time of one BB iteration's body and row passes on the
+        last solved system (CUDA events on the backend's stream)."""
+        body, row = c_float(0), c_float(0)
+        rows, bodies = c_uint64(0), c_uint64(0)
+        self._check(self._lib.msb_profile_iterations(self._handle, iterations, ctypes.byref(body), ctypes.byref(row),
+                                                     ctypes.byref(rows), ctypes.byref(bodies)))
+        return {"body_ms": body.value, "row_ms": row.value, "rows": rows.value, "bodies": bodies.value}
+
+    def _records(self, call, dtype, guess: int):
+        capacity = max(self._capacity, guess)
+        while True:
+            out = np.zeros(capacity, dtype=dtype)
+            count = c_uint64(0)
+            status = call(out, capacity, count)
+            if status == abi.ERR_CAPACITY:
+                capacity = int(count.value) + 16
+                continue
+            self._check(status)
+            self._capacity = max(self._capacity, int(count.value))
+            return out[: count.value].copy()
+
+    # -- ComputeBackend -------------------------------------------------
+    def find_cell_contacts(self, world, parameters: ContactParameters | None = None) -> np.ndarray:
+        """Contacts as ``abi.CELL_CONTACT_DTYPE`` records in (first id,
+        second id, ordinal) order."""
+        parameters = parameters or ContactParameters()
+        cells = world.arrays()
+        native = parameters.native()
+        return self._records(
+            lambda out, cap, count: self._lib.msb_find_cell_contacts(
+                self._handle, ctypes.byref(cells), ctypes.byref(native), c_void_p(abi.ptr(out)), cap,
+                ctypes.byref(count)),
+            abi.CELL_CONTACT_DTYPE,
+            8 * len(world),
+        )
+
+    def find_external_contacts(self, world, constraints, parameters: ConstraintContactParameters | None = None,
+                               every_face: bool = False) -> np.ndarray:
+        """find_external_contacts (nearest face) or, with ``every_face``,
+        find_external_contact_faces; ``abi.EXTERNAL_CONTACT_DTYPE`` records."""
+        parameters = parameters or ConstraintContactParameters()
+        cells = world.arrays()
+        native = parameters.native()
+        return self._records(
+            lambda out, cap, count: self._lib.msb_find_external_contacts(
+                self._handle, ctypes.byref(cells), c_void_p(constraints.pointer()), len(constraints),
+                ctypes.byref(native), 1 if every_face else 0, c_void_p(abi.ptr(out)), cap, ctypes.byref(count)),
+            abi.EXTERNAL_CONTACT_DTYPE,
+            4 * len(world) + 16,
+        )
+
+    def solve_contact_forces(self, system: ContactSystem, initial_multipliers,
+                             parameters: ContactSolveParameters | None = None) -> ContactSolveResult:
+        parameters = parameters or ContactSolveParameters()
+        native = system.native()
+        initial = np.ascontiguousarray(initial_multipliers, dtype=np.float32)
+        if initial.shape[0] != len(system.rows):
+            raise ValueError("contact multiplier count does not match the contact rows")
+        out = np.zeros(len(system.rows), dtype=np.float32)
+        report = abi.ContactSolveReport()
+        prm = parameters.native()
+        self._check(self._lib.msb_solve_contact_forces(
+            self._handle, ctypes.byref(native), c_void_p(abi.ptr(initial) if len(initial) else None),
+            ctypes.byref(prm), c_void_p(abi.ptr(out) if len(out) else None), ctypes.byref(report)))
+        if len(system.rows) == 0:
+            out = initial.copy()
+        return ContactSolveResult(out, ContactSolveReport(report.status, report.iterations, report.residual))
+
+    def evaluate_contact_response(self, system: ContactSystem, multipliers) -> ContactResponse:
+        native = system.native()
+        multipliers = np.ascontiguousarray(multipliers, dtype=np.float32)
+        if multipliers.shape[0] != len(system.rows):
+            raise ValueError("contact multiplier count does not match the contact rows")
+        n = len(system.bodies)
+        velocities = np.zeros((n, 6), dtype=np.float32)
+        loads = np.zeros(n, dtype=np.float32)
+        rates = np.zeros(n, dtype=np.float32)
+        self._check(self._lib.msb_evaluate_contact_response(
+            self._handle, ctypes.byref(native), c_void_p(abi.ptr(multipliers) if len(multipliers) else None),
+            c_void_p(abi.ptr(velocities)), c_void_p(abi.ptr(loads)), c_void_p(abi.ptr(rates))))
+        return ContactResponse(velocities, loads, rates)
+
+    def evaluate_contact_gaps(self, system: ContactSystem, multipliers) -> np.ndarray:
+        native = system.native()
+        multipliers = np.ascontiguousarray(multipliers, dtype=np.float32)
+        if multipliers.shape[0] != len(system.rows):
+            raise ValueError("contact multiplier count does not match the contact rows")
+        gaps = np.zeros(len(system.rows), dtype=np.float32)
+        self._check(self._lib.msb_evaluate_contact_gaps(
+            self._handle, ctypes.byref(native), c_void_p(abi.ptr(multipliers) if len(multipliers) else None),
+            c_void_p(abi.ptr(gaps) if len(gaps) else None)))
+        return gaps
+
+    def contact_system_diagonal_bound(self, system: ContactSystem) -> float:
+        native = system.native()
+        bound = c_float(0.0)
+        self._check(self._lib.msb_contact_system_diagonal_bound(self._handle, ctypes.byref(native),
+                                                               ctypes.byref(bound)))
+        return bound.value
+
+    def advance_contact_dynamics(self, world, constraints, dt: float,
+                                 dynamics: ContactDynamicsParameters | None = None,
+                                 contacts: ContactParameters | None = None,
+                                 constraint_parameters: ConstraintContactParameters | None = None,
+                                 ) -> ContactDynamicsResult:
+        """One contact-dynamics step of ``world`` (updated in place) with
+        host buffers: the upload, the step and the download in one call."""
+        dynamics = dynamics or ContactDynamicsParameters()
+        contacts = contacts or ContactParameters()
+        constraint_parameters = constraint_parameters or ConstraintContactParameters()
+        n = len(world)
+        cells = world.arrays()
+        velocities = np.zeros((n, 3), dtype=np.float32)
+        loads = np.zeros(n, dtype=np.float32)
+        increments = np.zeros(n, dtype=np.float32)
+        outputs = abi.ContactDynamicsOutputs(abi.ptr(velocities), abi.ptr(loads), abi.ptr(increments))
+        report = abi.ContactDynamicsReport()
+        dyn, cp, wp = dynamics.native(), contacts.native(), constraint_parameters.native()
+        pointer = constraints.pointer() if constraints is not None else None
+        count = len(constraints) if constraints is not None else 0
+        self._check(self._lib.msb_advance_contact_dynamics(
+            self._handle, ctypes.byref(cells), c_void_p(pointer), count, c_float(dt), ctypes.byref(dyn),
+            ctypes.byref(cp), ctypes.byref(wp), ctypes.byref(report), ctypes.byref(outputs)))
+        return ContactDynamicsResult(ContactDynamicsReport.from_native(report), velocities, loads, increments)
+
+    def advance_contact_dynamics_device(self, cells: "DeviceCells", constraints, dt: float,
+                                        dynamics: ContactDynamicsParameters | None = None,
+                                        contacts: ContactParameters | None = None,
+                                        constraint_parameters: ConstraintContactParameters | None = None,
+                                        outputs: "DeviceOutputs | None" = None) -> ContactDynamicsReport:
+        """The same step on cells held in device memory (``DeviceCells``)."""
+        dynamics = dynamics or ContactDynamicsParameters()
+        contacts = contacts or ContactParameters()
+        constraint_parameters = constraint_parameters or ConstraintContactParameters()
+        native_cells = cells.arrays()
+        native_outputs = outputs.native() if outputs is not None else None
+        report = abi.ContactDynamicsReport()
+        dyn, cp, wp = dynamics.native(), contacts.native(), constraint_parameters.native()
+        pointer = constraints.pointer() if constraints is not None else None
+        count = len(constraints) if constraints is not None else 0
+        self._check(self._lib.msb_advance_contact_dynamics_device(
+            self._handle, ctypes.byref(native_cells), c_void_p(pointer), count, c_float(dt), ctypes.byref(dyn),
+            ctypes.byref(cp), ctypes.byref(wp), ctypes.byref(report),
+            ctypes.byref(native_outputs) if native_outputs is not None else None))
+        return ContactDynamicsReport.from_native(report)
+
+
+class DeviceCells:
+    """A world's arrays resident in GPU memory (torch tensors used as
+    allocations only), for ``advance_contact_dynamics_device``."""
+
+    def __init__(self, world, device: str = "cuda:0"):
+        import torch
+
+        def up(array, dtype):
+            return torch.from_numpy(np.ascontiguousarray(array)).to(device=device, dtype=dtype)
+
+        self.count = len(world)
+        self.ids = up(world.ids.view(np.int64), torch.int64)
+        self.fields = {name: up(getattr(world, name), torch.float32) for name in world.FIELDS}
+        self.fixed = up(world.fixed, torch.uint8)
+
+    def arrays(self) -> abi.CellArrays:
+        f = self.fields
+        return abi.CellArrays(
+            self.count, self.ids.data_ptr(), f["position_x"].data_ptr(), f["position_y"].data_ptr(),
+            f["position_z"].data_ptr(), f["direction_x"].data_ptr(), f["direction_y"].data_ptr(),
+            f["direction_z"].data_ptr(), f["lengths"].data_ptr(), f["radii"].data_ptr(),
+            f["growth_rates"].data_ptr(), self.fixed.data_ptr())
+
+    def download(self, world) -> None:
+        for name in ("position_x", "position_y", "position_z", "direction_x", "direction_y", "direction_z",
+                     "lengths"):
+            setattr(world, name, self.fields[name].cpu().numpy().copy())
+
+
+class DeviceOutputs:
+    def __init__(self, count: int, device: str = "cuda:0"):
+        import torch
+
+        self.velocities = torch.zeros((count, 3), dtype=torch.float32, device=device)
+        self.loads = torch.zeros(count, dtype=torch.float32, device=device)
+        self.increments = torch.zeros(count, dtype=torch.float32, device=device)
+
+    def native(self) -> abi.ContactDynamicsOutputs:
+        return abi.ContactDynamicsOutputs(self.velocities.data_ptr(), self.loads.data_ptr(),
+                                          self.increments.data_ptr())

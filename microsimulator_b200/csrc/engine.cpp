@@ -1,0 +1,1218 @@
+// Host engine of the B200 contact backend (C++23).
+//
+// A context owns one non-blocking stream, device buffers that grow by powers
+// of two (as the reference's CudaBuffer does, cpp/cuda/cuda_backend.cu:40-88)
+// and the captured solve graphs.  Every per-cell, per-row and per-contact
+// pass runs on the device; the host keeps the substep controller of
+// detail::advance_contact_dynamics (cpp/core/contact_dynamics.cpp:676-782)
+// and reads a few scalars at its decision points.  The C-ABI entry points at
+// the end (declared in include/msb200.h) map exceptions to status codes.
+
+#include <algorithm>
+#include <array>
+#include <atomic>
+#include <bit>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <span>
+#include <stdexcept>
+#include <string>
+#include <utility>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/msb200.h"
+#include "kernels.h"
+#include "solve.h"
+#include "step.h"
+
+namespace msb {
+
+namespace {
+std::atomic<std::uint64_t> launches{0};
+}
+
+void count_launch(int n) { launches.fetch_add(std::uint64_t(n), std::memory_order_relaxed); }
+
+namespace {
+
+struct CudaError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct DeviceCheckError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+struct CapacityError : std::runtime_error {
+  using std::runtime_error::runtime_error;
+};
+
+void check(cudaError_t err, const char* what) {
+  if (err != cudaSuccess) {
+    throw CudaError(std::string(what) + ": " + cudaGetErrorString(err));
+  }
+}
+
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  std::size_t cap = 0;
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(std::exchange(o.p, nullptr)), cap(std::exchange(o.cap, 0)) {}
+  DBuf& operator=(DBuf&& o) noexcept {
+    std::swap(p, o.p);
+    std::swap(cap, o.cap);
+    return *this;
+  }
+  ~DBuf() { release(); }
+  void release() {
+    if (p != nullptr) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+  // Grows to at least n elements; contents are not kept.
+  T* ensure(std::size_t n) {
+    if (n > cap) {
+      release();
+      const std::size_t c = std::bit_ceil(std::max<std::size_t>(n, 64));
+      check(cudaMalloc(&p, c * sizeof(T)), "cudaMalloc");
+      cap = c;
+    }
+    return p;
+  }
+  // Grows to at least n elements keeping the first `keep`.
+  T* grow(std::size_t n, std::size_t keep, cudaStream_t stream) {
+    if (n <= cap) return p;
+    const std::size_t c = std::bit_ceil(std::max<std::size_t>(n, 64));
+    T* q = nullptr;
+    check(cudaMalloc(&q, c * sizeof(T)), "cudaMalloc");
+    if (keep > 0) check(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, stream), "grow copy");
+    check(cudaStreamSynchronize(stream), "grow");
+    release();
+    p = q;
+    cap = c;
+    return p;
+  }
+};
+
+struct Geometry {
+  DBuf<float4> pos_len;
+  DBuf<float4> dir_rad;
+  GeometryBuffers view() { return {pos_len.p, dir_rad.p}; }
+  void ensure(std::size_t n) {
+    pos_len.ensure(n);
+    dir_rad.ensure(n);
+  }
+};
+
+// The rows of one substep with their keys, multipliers and keyed lists.
+struct RowStore {
+  DBuf<float4> a, b, c, d;
+  DBuf<uint2> slots;
+  DBuf<std::uint64_t> partner;
+  DBuf<float> multipliers;
+  DBuf<float> gaps;
+  DBuf<std::uint32_t> keyed_offsets;
+  DBuf<std::uint32_t> keyed_rows;
+  std::uint32_t count = 0;
+
+  RowArrays arrays() { return {a.p, b.p, c.p, d.p, slots.p}; }
+  void ensure(std::size_t n) {
+    a.ensure(n);
+    b.ensure(n);
+    c.ensure(n);
+    d.ensure(n);
+    slots.ensure(n);
+    partner.ensure(n);
+    multipliers.ensure(n);
+    gaps.ensure(n);
+  }
+  void grow(std::size_t n, cudaStream_t s) {
+    a.grow(n, count, s);
+    b.grow(n, count, s);
+    c.grow(n, count, s);
+    d.grow(n, count, s);
+    slots.grow(n, count, s);
+    partner.grow(n, count, s);
+    multipliers.grow(n, count, s);
+    gaps.grow(n, count, s);
+  }
+  KeyedLists keyed() const { return {keyed_offsets.p, keyed_rows.p, partner.p, multipliers.p}; }
+};
+
+// Small scalars read back at the controller's decision points.
+enum Scalar : int {
+  kStatus = 0,
+  kOverlapBits = 1,
+  kRotationBits = 2,
+  kInvalid = 3,
+  kGrowthBits = 4,
+  kScalarCount = 16
+};
+
+struct SolveOutcome {
+  std::uint32_t status = MSB_SOLVE_CONVERGED;
+  std::uint32_t iterations = 0;
+  float residual = 0.0f;
+};
+
+constexpr std::uint32_t kRotationProbeIterations = 128;
+constexpr float kSolveToleranceFraction = 0.25f;
+constexpr float kLoadResolutionFraction = 0.1f;
+constexpr std::uint32_t kEasyRefinements = 2;
+constexpr float kMaximumSubstepRotation = 0.5f;
+constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
+
+bool positive(float v) { return std::isfinite(v) && v > 0.0f; }
+
+void validate_contact_parameters(const msb_contact_parameters& p) {
+  if (!std::isfinite(p.activation_margin) || p.activation_margin < 0.0f) {
+    throw std::invalid_argument("contact activation margin must be finite and non-negative");
+  }
+  if (!std::isfinite(p.parallel_sine_threshold) || p.parallel_sine_threshold < 0.0f ||
+      p.parallel_sine_threshold > 1.0f) {
+    throw std::invalid_argument("contact parallel threshold must be between zero and one");
+  }
+  if (!positive(p.degeneracy_epsilon)) {
+    throw std::invalid_argument("contact degeneracy epsilon must be finite and positive");
+  }
+}
+
+void validate_constraint_parameters(const msb_constraint_contact_parameters& p) {
+  if (!std::isfinite(p.activation_margin) || p.activation_margin < 0.0f) {
+    throw std::invalid_argument("constraint activation margin must be finite and non-negative");
+  }
+  if (!positive(p.degeneracy_epsilon)) {
+    throw std::invalid_argument("constraint degeneracy epsilon must be finite and positive");
+  }
+}
+
+void validate_growth(const msb_growth_load_response& g) {
+  if (g.law > MSB_GROWTH_LAW_LINEAR) throw std::invalid_argument("growth load law is invalid");
+  if (!std::isfinite(g.sensitivity) || g.sensitivity < 0.0f) {
+    throw std::invalid_argument("growth load sensitivity must be finite and non-negative");
+  }
+  if (!std::isfinite(g.free_load) || !std::isfinite(g.stall_load) || g.free_load < 0.0f ||
+      g.stall_load <= g.free_load) {
+    throw std::invalid_argument("growth stall load must be finite and exceed a finite, non-negative free load");
+  }
+}
+
+void validate_dynamics(const msb_contact_dynamics_parameters& p) {
+  if (!positive(p.drag)) throw std::invalid_argument("contact dynamics drag must be finite and positive");
+  if (!positive(p.contact_stiffness) || !positive(p.wall_stiffness)) {
+    throw std::invalid_argument("contact and wall stiffness must be finite and positive");
+  }
+  if (!positive(p.overlap_tolerance)) {
+    throw std::invalid_argument("contact overlap tolerance must be finite and positive");
+  }
+  if (!std::isfinite(p.candidate_margin) || p.candidate_margin < 0.0f) {
+    throw std::invalid_argument("contact candidate margin must be finite and non-negative");
+  }
+  if (!positive(p.max_overlap_recovery)) {
+    throw std::invalid_argument("contact overlap recovery must be finite and positive");
+  }
+  if (!positive(p.max_growth_fraction)) {
+    throw std::invalid_argument("contact growth fraction must be finite and positive");
+  }
+  if (p.max_iterations == 0) throw std::invalid_argument("contact dynamics iteration limit must be positive");
+  if (p.flow_drift != 0) {
+    throw std::invalid_argument("flow drift inside the contact solve is not supported by this backend");
+  }
+  validate_growth(p.growth);
+}
+
+float effective_overlap_tolerance(const msb_contact_dynamics_parameters& p) {
+  float load_scale = 0.0f;
+  if (p.growth.law == MSB_GROWTH_LAW_LINEAR) {
+    load_scale = p.growth.stall_load - p.growth.free_load;
+  } else if (p.growth.law == MSB_GROWTH_LAW_EXPONENTIAL && p.growth.sensitivity > 0.0f) {
+    load_scale = 1.0f / p.growth.sensitivity;
+  }
+  if (load_scale <= 0.0f) return p.overlap_tolerance;
+  return std::min(p.overlap_tolerance, kLoadResolutionFraction * load_scale / p.contact_stiffness);
+}
+
+bool finite_row(const msb_contact_row& r) {
+  bool ok = std::isfinite(r.offset) && std::isfinite(r.compliance) && r.compliance >= 0.0f &&
+            std::isfinite(r.first_length_lever) && std::isfinite(r.second_length_lever) &&
+            r.first_length_lever >= 0.0f && r.second_length_lever >= 0.0f;
+  for (int k = 0; k < 6; ++k) ok = ok && std::isfinite(r.first_jacobian[k]) && std::isfinite(r.second_jacobian[k]);
+  return ok;
+}
+
+// validate_contact_system (contact_dynamics.cpp:640-672) on the host records.
+void validate_system(const msb_contact_system& s) {
+  if (!std::isfinite(s.dt) || s.dt <= 0.0f) {
+    throw std::invalid_argument("contact system time step must be finite and positive");
+  }
+  validate_growth(s.growth);
+  if (s.body_count > 0xFFFFFFF0ull || s.row_count > 0x7FFFFFF0ull) {
+    throw std::overflow_error("contact system has too many rows or bodies");
+  }
+  for (std::uint64_t i = 0; i < s.body_count; ++i) {
+    const auto& b = s.bodies[i];
+    bool ok = std::isfinite(b.axis.x) && std::isfinite(b.axis.y) && std::isfinite(b.axis.z) &&
+              std::isfinite(b.translational_mobility) && std::isfinite(b.transverse_mobility) &&
+              std::isfinite(b.axial_mobility) && std::isfinite(b.length_rate) && b.translational_mobility >= 0.0f &&
+              b.transverse_mobility >= 0.0f && b.axial_mobility >= 0.0f;
+    for (float v : b.drift) ok = ok && std::isfinite(v);
+    if (!ok) throw std::invalid_argument("contact body is invalid");
+  }
+  for (std::uint64_t i = 0; i < s.row_count; ++i) {
+    const auto& r = s.rows[i];
+    if (r.first_slot >= s.body_count || (r.second_slot != kInvalidSlot && r.second_slot >= s.body_count)) {
+      throw std::invalid_argument("contact row slot is out of range");
+    }
+    if (!finite_row(r)) throw std::invalid_argument("contact row is invalid");
+  }
+}
+
+void require_multipliers(const float* m, std::uint64_t n) {
+  for (std::uint64_t i = 0; i < n; ++i) {
+    if (!std::isfinite(m[i]) || m[i] < 0.0f) {
+      throw std::invalid_argument("contact multipliers must be finite and non-negative");
+    }
+  }
+}
+
+}  // namespace
+}  // namespace msb
+
+struct msb_context {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  std::string error;
+  std::string device_name;
+  std::uint64_t launches_at_create = 0;
+
+  // cells
+  std::uint32_t n = 0;
+  msb::DBuf<std::uint64_t> ids;
+  msb::DBuf<float> growth;
+  msb::DBuf<std::uint8_t> fixed;
+  std::array<msb::DBuf<float>, 8> staging;  // px, py, pz, dx, dy, dz, len, radius
+  msb::Geometry state, base, initial, trial;
+  msb::DBuf<std::uint32_t> order, rank;
+
+  // scratch for scans and sorts
+  msb::DBuf<std::uint32_t> temp, sort_keys, sort_values, counts;
+
+  // contact search
+  msb::DBuf<double> bounds, bound_partials;
+  msb::DBuf<msb::GridParams> grid;
+  msb::DBuf<std::uint32_t> cell_bucket, bucket_counts, bucket_starts, bucket_fill, members;
+  msb::DBuf<std::int64_t> coords;
+  msb::DBuf<std::uint32_t> cand_counts, cand_offsets, pair_counts, pair_offsets, wall_counts, wall_offsets;
+  msb::DBuf<uint2> pairs;
+  msb::DBuf<msb::Touch> touches, found, flagged;
+  msb::DBuf<std::uint32_t> flags, flag_offsets;
+  msb::DBuf<msb::DeviceConstraint> constraints;
+  std::uint32_t constraint_count = 0;
+
+  // the contact system
+  msb::RowStore rows, memory;
+  bool has_memory = false;
+  msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
+  msb::DBuf<std::uint32_t> inc_offsets;
+  msb::DBuf<float4> inc_a, inc_b, resp_a, resp_b, accepted_a, accepted_b;
+  msb::DBuf<float> slack;
+
+  // solve
+  int last_blocks = 0;
+  msb::SolveDesc* desc = nullptr;
+  msb::DBuf<double> partials;
+  std::vector<std::unique_ptr<msb::SolveGraph>> graphs;
+
+  // scalars
+  msb::DBuf<std::uint32_t> scalars;
+  std::uint32_t* host_scalars = nullptr;
+  msb::SolveDesc* host_desc = nullptr;
+
+  // outputs staging for host calls
+  msb::DBuf<float> out_velocities, out_loads, out_increments;
+  msb::DBuf<std::uint8_t> records;
+};
+
+namespace msb {
+namespace {
+
+using Ctx = msb_context;
+
+void sync(Ctx& c) { check(cudaStreamSynchronize(c.stream), "stream"); }
+
+// Clears the scalar words except the status word, which keeps the first
+// failure until read_scalars reports it.
+void reset_scalars(Ctx& c) {
+  check(cudaMemsetAsync(c.scalars.p + 1, 0, (kScalarCount - 1) * 4, c.stream), "memset");
+}
+
+void reset_status(Ctx& c) { check(cudaMemsetAsync(c.scalars.p, 0, kScalarCount * 4, c.stream), "memset"); }
+
+void read_scalars(Ctx& c) {
+  check(cudaMemcpyAsync(c.host_scalars, c.scalars.p, kScalarCount * 4, cudaMemcpyDeviceToHost, c.stream), "read");
+  sync(c);
+  if (c.host_scalars[kStatus] != kStatusOk) {
+    const auto code = c.host_scalars[kStatus];
+    if (code == kStatusGeometry) throw std::invalid_argument("cell geometry is invalid (non-finite, negative or unnormalized)");
+    if (code == kStatusIndex) throw std::invalid_argument("cell identifiers must be non-zero and unique");
+    throw DeviceCheckError("a device-side check failed (code " + std::to_string(code) + ")");
+  }
+}
+
+float bits_to_float(std::uint32_t bits) {
+  float f;
+  std::memcpy(&f, &bits, 4);
+  return f;
+}
+
+std::uint32_t read_u32(Ctx& c, const std::uint32_t* device_ptr) {
+  std::uint32_t v = 0;
+  check(cudaMemcpyAsync(c.host_scalars + kScalarCount, device_ptr, 4, cudaMemcpyDeviceToHost, c.stream), "read");
+  sync(c);
+  v = c.host_scalars[kScalarCount];
+  return v;
+}
+
+GeometryView view_of(Ctx& c, Geometry& g) { return {g.pos_len.p, g.dir_rad.p, c.ids.p, c.n}; }
+
+// ---- cells ---------------------------------------------------------------
+
+void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
+  if (cells.count >= 0xFFFFFFF0ull) throw std::overflow_error("cell count exceeds the slot index space");
+  if (cells.count > 0 && (cells.ids == nullptr || cells.position_x == nullptr || cells.position_y == nullptr ||
+                          cells.position_z == nullptr || cells.direction_x == nullptr ||
+                          cells.direction_y == nullptr || cells.direction_z == nullptr || cells.lengths == nullptr ||
+                          cells.radii == nullptr)) {
+    throw std::invalid_argument("cell arrays must not be null");
+  }
+  c.n = std::uint32_t(cells.count);
+  const std::size_t n = c.n;
+  if (n == 0) return;
+  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+  c.ids.ensure(n);
+  c.growth.ensure(n);
+  c.fixed.ensure(n);
+  check(cudaMemcpyAsync(c.ids.p, cells.ids, n * 8, kind, c.stream), "copy ids");
+  const float* src[8] = {cells.position_x,  cells.position_y,  cells.position_z, cells.direction_x,
+                         cells.direction_y, cells.direction_z, cells.lengths,    cells.radii};
+  for (int k = 0; k < 8; ++k) {
+    c.staging[k].ensure(n);
+    check(cudaMemcpyAsync(c.staging[k].p, src[k], n * 4, kind, c.stream), "copy cells");
+  }
+  if (cells.growth_rates != nullptr) {
+    check(cudaMemcpyAsync(c.growth.p, cells.growth_rates, n * 4, kind, c.stream), "copy growth");
+  } else {
+    check(cudaMemsetAsync(c.growth.p, 0, n * 4, c.stream), "memset");
+  }
+  if (cells.fixed != nullptr) {
+    check(cudaMemcpyAsync(c.fixed.p, cells.fixed, n, kind, c.stream), "copy fixed");
+  } else {
+    check(cudaMemsetAsync(c.fixed.p, 0, n, c.stream), "memset");
+  }
+  c.state.ensure(n);
+  reset_status(c);
+  launch_pack_cells(c.n, c.staging[0].p, c.staging[1].p, c.staging[2].p, c.staging[3].p, c.staging[4].p,
+                    c.staging[5].p, c.staging[6].p, c.staging[7].p, c.state.view(), c.scalars.p + kStatus, c.stream);
+
+  // Id order: LSD radix sort of the ids (low word, then high word if used).
+  c.order.ensure(n);
+  c.rank.ensure(n);
+  c.sort_keys.ensure(n);
+  c.temp.ensure(sort_temp_words(n) + scan_temp_words(4 * n + 8192) + 64);
+  launch_max_u64(c.ids.p, c.n, reinterpret_cast<std::uint64_t*>(c.scalars.p + 8), c.stream);
+  read_scalars(c);
+  std::uint64_t max_id = 0;
+  std::memcpy(&max_id, c.host_scalars + 8, 8);
+  const int bits = max_id == 0 ? 1 : 64 - std::countl_zero(max_id);
+  iota(c.order.p, n, c.stream);
+  launch_id_low_words(c.ids.p, c.n, 0, nullptr, c.sort_keys.p, c.stream);
+  radix_sort_pairs(c.sort_keys.p, c.order.p, n, std::min(bits, 32), c.temp.p, c.stream);
+  if (bits > 32) {
+    launch_id_low_words(c.ids.p, c.n, 32, c.order.p, c.sort_keys.p, c.stream);
+    radix_sort_pairs(c.sort_keys.p, c.order.p, n, bits - 32, c.temp.p, c.stream);
+  }
+  launch_invert_permutation(c.order.p, c.n, c.rank.p, c.stream);
+  launch_check_unique_ids(c.ids.p, c.order.p, c.n, c.scalars.p + kStatus, c.stream);
+  read_scalars(c);
+}
+
+void load_constraints(Ctx& c, const msb_constraint* constraints, std::uint64_t count) {
+  if (count > 0 && constraints == nullptr) throw std::invalid_argument("constraint array must not be null");
+  std::vector<DeviceConstraint> sorted(count);
+  for (std::uint64_t i = 0; i < count; ++i) {
+    const auto& k = constraints[i];
+    if (k.kind > MSB_CONSTRAINT_CYLINDER) throw std::invalid_argument("constraint kind is invalid");
+    if (k.id == 0) throw std::invalid_argument("constraint identifier is invalid");
+    static_assert(sizeof(DeviceConstraint) == sizeof(msb_constraint));
+    std::memcpy(&sorted[i], &k, sizeof(k));
+  }
+  // Within a cell, the reference emits planes, spheres, boxes and cylinders in
+  // insertion order and then sorts stably by constraint id; ids are unique,
+  // so sorting the constraints by id gives the same order.
+  std::stable_sort(sorted.begin(), sorted.end(), [](const auto& l, const auto& r) { return l.id < r.id; });
+  for (std::size_t i = 1; i < sorted.size(); ++i) {
+    if (sorted[i].id == sorted[i - 1].id) throw std::invalid_argument("constraint identifiers must be unique");
+  }
+  c.constraint_count = std::uint32_t(count);
+  if (count > 0) {
+    c.constraints.ensure(count);
+    check(cudaMemcpyAsync(c.constraints.p, sorted.data(), count * sizeof(DeviceConstraint), cudaMemcpyHostToDevice,
+                          c.stream),
+          "copy constraints");
+    sync(c);
+  }
+}
+
+// ---- contact search ------------------------------------------------------
+
+// Cell-pair touches of `geometry` into c.touches[0, count); returns count.
+std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DBuf<Touch>& out) {
+  const std::uint32_t n = c.n;
+  if (n < 2) return 0;
+  const GeometryView g = view_of(c, geometry);
+  const std::uint32_t partials = bound_partials(n);
+  c.bounds.ensure(6ull * n);
+  c.bound_partials.ensure(10ull * partials);
+  c.grid.ensure(1);
+  launch_cell_bounds(g, prm.margin, c.bounds.p, c.bound_partials.p, c.stream);
+  const std::uint64_t capacity = grid_bucket_capacity(n);
+  launch_grid_setup(c.bound_partials.p, partials, n, capacity, c.grid.p, c.stream);
+  c.cell_bucket.ensure(n);
+  c.coords.ensure(3ull * n);
+  c.bucket_counts.ensure(capacity);
+  c.bucket_starts.ensure(capacity);
+  c.bucket_fill.ensure(capacity);
+  c.members.ensure(n);
+  c.temp.ensure(scan_temp_words(capacity) + sort_temp_words(n) + 64);
+  check(cudaMemsetAsync(c.bucket_counts.p, 0, capacity * 4, c.stream), "memset");
+  check(cudaMemsetAsync(c.bucket_fill.p, 0, capacity * 4, c.stream), "memset");
+  launch_bin_cells(g, c.bounds.p, c.grid.p, c.cell_bucket.p, c.coords.p, c.bucket_counts.p, c.stream);
+  exclusive_scan(c.bucket_counts.p, c.bucket_starts.p, capacity, c.temp.p, c.stream);
+  launch_scatter_cells(n, c.cell_bucket.p, c.bucket_starts.p, c.bucket_fill.p, c.members.p, c.stream);
+  c.cand_counts.ensure(n + 1ull);
+  c.cand_offsets.ensure(n + 1ull);
+  check(cudaMemsetAsync(c.cand_counts.p + n, 0, 4, c.stream), "memset");
+  reset_scalars(c);
+  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.members.p, c.coords.p, c.rank.p, c.cand_counts.p,
+                     nullptr, nullptr, c.scalars.p + kStatus, c.stream);
+  exclusive_scan(c.cand_counts.p, c.cand_offsets.p, n + 1ull, c.temp.p, c.stream);
+  // grid status and the candidate total
+  GridParams grid{};
+  check(cudaMemcpyAsync(&c.host_scalars[kScalarCount + 2], c.cand_offsets.p + n, 4, cudaMemcpyDeviceToHost, c.stream),
+        "read");
+  check(cudaMemcpyAsync(&grid, c.grid.p, sizeof(GridParams), cudaMemcpyDeviceToHost, c.stream), "read grid");
+  read_scalars(c);
+  if (grid.status == 1) throw std::invalid_argument("cell geometry is not finite");
+  if (grid.status != 0) throw DeviceCheckError("grid bucket capacity exceeded");
+  const std::uint32_t pair_count = c.host_scalars[kScalarCount + 2];
+  if (pair_count == 0) return 0;
+  c.pairs.ensure(pair_count);
+  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.members.p, c.coords.p, c.rank.p, c.cand_counts.p,
+                     c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus, c.stream);
+  c.pair_counts.ensure(pair_count + 1ull);
+  c.pair_offsets.ensure(pair_count + 1ull);
+  c.temp.ensure(scan_temp_words(pair_count + 1ull) + scan_temp_words(capacity) + sort_temp_words(n) + 64);
+  check(cudaMemsetAsync(c.pair_counts.p + pair_count, 0, 4, c.stream), "memset");
+  launch_narrow_phase(g, c.pairs.p, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream);
+  exclusive_scan(c.pair_counts.p, c.pair_offsets.p, pair_count + 1ull, c.temp.p, c.stream);
+  const std::uint32_t touch_count = read_u32(c, c.pair_offsets.p + pair_count);
+  read_scalars(c);
+  if (touch_count == 0) return 0;
+  out.ensure(touch_count + 1ull);
+  launch_narrow_phase(g, c.pairs.p, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream);
+  return touch_count;
+}
+
+// Wall touches appended at out[base, base + count); returns count.
+std::uint32_t find_walls(Ctx& c, Geometry& geometry, float margin, float epsilon, bool every_face, DBuf<Touch>& out,
+                         std::uint32_t base) {
+  const std::uint32_t n = c.n;
+  if (n == 0 || c.constraint_count == 0) return 0;
+  const GeometryView g = view_of(c, geometry);
+  c.wall_counts.ensure(n + 1ull);
+  c.wall_offsets.ensure(n + 1ull);
+  c.temp.ensure(scan_temp_words(n + 1ull) + 64);
+  check(cudaMemsetAsync(c.wall_counts.p + n, 0, 4, c.stream), "memset");
+  launch_wall_contacts(g, c.constraints.p, c.constraint_count, margin, epsilon, every_face ? 1u : 0u, c.rank.p,
+                       c.wall_counts.p, nullptr, nullptr, c.stream);
+  exclusive_scan(c.wall_counts.p, c.wall_offsets.p, n + 1ull, c.temp.p, c.stream);
+  const std::uint32_t count = read_u32(c, c.wall_offsets.p + n);
+  if (count == 0) return 0;
+  out.grow(std::size_t(base) + count + 1, base, c.stream);
+  launch_wall_contacts(g, c.constraints.p, c.constraint_count, margin, epsilon, every_face ? 1u : 0u, c.rank.p,
+                       nullptr, c.wall_offsets.p, out.p + base, c.stream);
+  return count;
+}
+
+// find_touches (contact_dynamics.cpp:176-210): pairs then constraint faces.
+std::uint32_t find_touches(Ctx& c, Geometry& geometry, const msb_contact_parameters& cp,
+                           const msb_constraint_contact_parameters& wp, float margin, DBuf<Touch>& out) {
+  const ContactSearchParams prm{margin, cp.parallel_sine_threshold, cp.degeneracy_epsilon};
+  const std::uint32_t pairs = find_pairs(c, geometry, prm, out);
+  const std::uint32_t walls = find_walls(c, geometry, margin, wp.degeneracy_epsilon, true, out, pairs);
+  return pairs + walls;
+}
+
+// ---- solve ---------------------------------------------------------------
+
+SolveGraph& graph_for(Ctx& c, std::uint32_t items) {
+  static constexpr int classes[] = {1, 4, 16, 74, 148, 592, 1184};
+  const std::uint32_t wanted = (items + kSolveThreads - 1) / kSolveThreads;
+  int index = 0;
+  while (index + 1 < int(std::size(classes)) && std::uint32_t(classes[index]) < wanted) ++index;
+  if (c.graphs.size() < std::size(classes)) c.graphs.resize(std::size(classes));
+  auto& slot = c.graphs[index];
+  if (!slot) {
+    slot = std::make_unique<SolveGraph>();
+    check(cudaError_t(slot->create(c.desc, classes[index], c.stream)), "solve graph");
+  }
+  return *slot;
+}
+
+void fill_desc(Ctx& c, std::uint32_t row_count, float dt, const msb_growth_load_response& growth, float tolerance,
+               std::uint32_t max_iterations) {
+  SolveDesc& d = *c.host_desc;
+  d.rows = c.rows.arrays();
+  d.bodies = {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
+  d.incidence = {c.inc_offsets.p, c.inc_a.p, c.inc_b.p};
+  d.response = {c.resp_a.p, c.resp_b.p};
+  d.multipliers = c.rows.multipliers.p;
+  d.gaps = c.rows.gaps.p;
+  d.partials = c.partials.p;
+  d.row_count = row_count;
+  d.body_count = c.n;
+  d.dt = dt;
+  d.law = growth.law;
+  d.sensitivity = growth.sensitivity;
+  d.free_load = growth.free_load;
+  d.stall_load = growth.stall_load;
+  d.tolerance = tolerance;
+  d.max_iterations = max_iterations;
+  // Copy only the problem part; the state part is reset in the graph.
+  check(cudaMemcpyAsync(c.desc, &d, offsetof(SolveDesc, step), cudaMemcpyHostToDevice, c.stream), "desc");
+}
+
+void build_system_incidence(Ctx& c, std::uint32_t row_count) {
+  const std::size_t entries = 2ull * std::max<std::uint32_t>(row_count, 1);
+  c.inc_offsets.ensure(c.n + 1ull);
+  c.inc_a.ensure(entries);
+  c.inc_b.ensure(entries);
+  c.sort_keys.ensure(entries);
+  c.sort_values.ensure(entries);
+  c.counts.ensure(c.n + 1ull);
+  c.temp.ensure(sort_temp_words(entries) + scan_temp_words(c.n + 1ull) + 64);
+  build_incidence(c.rows.arrays(), row_count, c.n, {c.inc_offsets.p, c.inc_a.p, c.inc_b.p}, c.sort_keys.p,
+                  c.sort_values.p, c.counts.p, c.temp.p, c.stream);
+}
+
+void build_row_keys(Ctx& c, RowStore& store) {
+  c.sort_keys.ensure(std::max<std::uint32_t>(store.count, 1));
+  c.counts.ensure(c.n + 1ull);
+  store.keyed_offsets.ensure(c.n + 1ull);
+  store.keyed_rows.ensure(std::max<std::uint32_t>(store.count, 1));
+  c.temp.ensure(sort_temp_words(store.count + 1ull) + scan_temp_words(c.n + 1ull) + 64);
+  build_keyed(store.slots.p, store.count, c.n, store.keyed_offsets.p, store.keyed_rows.p, c.sort_keys.p, c.counts.p,
+              c.temp.p, c.stream);
+}
+
+// Runs the solve graph on c.rows (multipliers in place).  Requires the
+// incidence of c.rows and the bodies.
+SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, float tolerance,
+                   std::uint32_t max_iterations) {
+  const std::uint32_t rows = c.rows.count;
+  c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
+  if (rows == 0) {
+    fill_desc(c, 0, dt, growth, tolerance, max_iterations);
+    launch_evaluate(c.desc, std::max(1, grid_for(c.n, kSolveThreads)), false, c.stream);
+    return {};
+  }
+  auto& graph = graph_for(c, std::max(rows, c.n));
+  c.last_blocks = graph.blocks();
+  c.partials.ensure(5ull * 1184);
+  fill_desc(c, rows, dt, growth, tolerance, max_iterations);
+  check(cudaError_t(graph.launch(c.stream)), "solve launch");
+  check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read desc");
+  sync(c);
+  const SolveDesc& d = *c.host_desc;
+  count_launch(int(2 * d.iterations));
+  if (d.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
+  return {d.status, d.iterations, d.residual};
+}
+
+// ---- the substep and the step -------------------------------------------
+
+struct Attempt {
+  bool accepted = false;
+  float rotation = 0.0f;
+  std::uint32_t refinements = 0;
+  std::uint32_t rows = 0;
+  float max_overlap = 0.0f;
+};
+
+Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, const msb_contact_parameters& cp,
+                        const msb_constraint_contact_parameters& wp, bool probe, std::uint64_t& iterations) {
+  const std::uint32_t n = c.n;
+  c.body_a.ensure(n);
+  c.body_b.ensure(n);
+  c.drift_a.ensure(n);
+  c.drift_b.ensure(n);
+  launch_make_bodies(n, c.state.view(), c.growth.p, c.fixed.p, c.initial.view(), p.drag,
+                     {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream);
+  const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches);
+  c.rows.count = 0;
+  c.rows.ensure(std::max<std::uint32_t>(found, 1));
+  reset_scalars(c);
+  const RowBuild build{p.wall_stiffness, p.contact_stiffness, p.max_overlap_recovery, dt};
+  launch_make_rows(c.touches.p, found, c.base.view(), build, nullptr, c.rows.arrays(), 0, c.rows.partner.p,
+                   c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
+  c.rows.count = found;
+  const float tolerance = effective_overlap_tolerance(p);
+  c.slack.ensure(1);
+  launch_slack(c.scalars.p + kOverlapBits, tolerance, p.max_overlap_recovery, c.slack.p, c.stream);
+  build_row_keys(c, c.rows);
+  const KeyedLists memory = c.memory.keyed();
+  launch_warm_start(found, c.rows.slots.p, c.rows.keyed(), c.has_memory ? &memory : nullptr, c.rows.multipliers.p,
+                    c.stream);
+  const float solve_tolerance = kSolveToleranceFraction * tolerance;
+  Attempt attempt;
+  for (std::uint32_t refinement = 0; refinement <= p.max_refinements; ++refinement) {
+    build_system_incidence(c, c.rows.count);
+    std::uint32_t remaining = p.max_iterations;
+    bool solved = false;
+    if (probe && refinement == 0 && remaining > kRotationProbeIterations) {
+      const auto early = solve(c, dt, p.growth, solve_tolerance, kRotationProbeIterations);
+      iterations += early.iterations;
+      remaining -= early.iterations;
+      if (early.status == MSB_SOLVE_BREAKDOWN) break;
+      if (early.status != MSB_SOLVE_CONVERGED) {
+        reset_scalars(c);
+        launch_largest_rotation(n, {c.resp_a.p, c.resp_b.p}, dt, c.scalars.p + kRotationBits, c.stream);
+        read_scalars(c);
+        attempt.rotation = bits_to_float(c.host_scalars[kRotationBits]);
+        if (attempt.rotation > kMaximumSubstepRotation) break;
+      } else {
+        // A second solve from converged multipliers takes no iteration.
+        solved = true;
+      }
+    }
+    if (!solved) {
+      const auto full = solve(c, dt, p.growth, solve_tolerance, remaining);
+      iterations += full.iterations;
+      if (full.status != MSB_SOLVE_CONVERGED) break;
+    }
+    // Move from the base geometry under the response of the solution.
+    c.trial.ensure(n);
+    reset_scalars(c);
+    launch_move(n, c.base.view(), {c.resp_a.p, c.resp_b.p}, dt, c.trial.view(), c.scalars.p + kRotationBits,
+                c.scalars.p + kInvalid, c.scalars.p + kStatus, c.stream);
+    read_scalars(c);
+    attempt.rotation = bits_to_float(c.host_scalars[kRotationBits]);
+    if (c.host_scalars[kInvalid] != 0) break;
+    launch_restore(n, c.trial.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
+
+    const std::uint32_t overlapping_candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
+    c.flags.ensure(overlapping_candidates + 1ull);
+    c.flag_offsets.ensure(overlapping_candidates + 1ull);
+    reset_scalars(c);
+    check(cudaMemsetAsync(c.flags.p + overlapping_candidates, 0, 4, c.stream), "memset");
+    launch_recheck(c.found.p, overlapping_candidates, c.rows.keyed(), c.slack.p, p.wall_stiffness,
+                   p.contact_stiffness, c.flags.p, c.scalars.p + kOverlapBits, c.stream);
+    c.temp.ensure(scan_temp_words(overlapping_candidates + 1ull) + 64);
+    exclusive_scan(c.flags.p, c.flag_offsets.p, overlapping_candidates + 1ull, c.temp.p, c.stream);
+    check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 4, c.flag_offsets.p + overlapping_candidates, 4,
+                          cudaMemcpyDeviceToHost, c.stream),
+          "read");
+    read_scalars(c);
+    const std::uint32_t overlapping = c.host_scalars[kScalarCount + 4];
+    const float max_overlap = bits_to_float(c.host_scalars[kOverlapBits]);
+    if (overlapping == 0) {
+      attempt.accepted = true;
+      attempt.refinements = refinement;
+      attempt.rows = c.rows.count;
+      attempt.max_overlap = max_overlap;
+      return attempt;
+    }
+    // Rows for the new overlaps, linearized at the trial geometry, with
+    // offsets that the multipliers of the move predict (contact_dynamics.cpp:567-578).
+    c.flagged.ensure(overlapping);
+    launch_gather_flagged(c.found.p, overlapping_candidates, c.flags.p, c.flag_offsets.p, c.flagged.p, c.stream);
+    const std::uint32_t base_row = c.rows.count;
+    c.rows.grow(std::size_t(base_row) + overlapping, c.stream);
+    const ResponseArrays response{c.resp_a.p, c.resp_b.p};
+    launch_make_rows(c.flagged.p, overlapping, c.trial.view(), build, &response, c.rows.arrays(), base_row,
+                     c.rows.partner.p, c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
+    c.rows.count = base_row + overlapping;
+    build_row_keys(c, c.rows);
+  }
+  launch_restore(n, c.base.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
+  reset_scalars(c);
+  attempt.accepted = false;
+  return attempt;
+}
+
+void copy_geometry(Ctx& c, Geometry& dst, Geometry& src) {
+  dst.ensure(c.n);
+  check(cudaMemcpyAsync(dst.pos_len.p, src.pos_len.p, c.n * sizeof(float4), cudaMemcpyDeviceToDevice, c.stream), "copy");
+  check(cudaMemcpyAsync(dst.dir_rad.p, src.dir_rad.p, c.n * sizeof(float4), cudaMemcpyDeviceToDevice, c.stream), "copy");
+}
+
+struct StepOutcome {
+  msb_contact_dynamics_report report{};
+};
+
+// detail::advance_contact_dynamics (contact_dynamics.cpp:676-782) over the
+// cells loaded in c.state.  Leaves the final geometry in c.state and the
+// outputs in c.out_*.
+StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, const msb_contact_parameters& cp,
+                    const msb_constraint_contact_parameters& wp) {
+  StepOutcome out;
+  const std::uint32_t n = c.n;
+  c.out_velocities.ensure(3ull * std::max<std::uint32_t>(n, 1));
+  c.out_loads.ensure(std::max<std::uint32_t>(n, 1));
+  c.out_increments.ensure(std::max<std::uint32_t>(n, 1));
+  if (n == 0) return out;
+  check(cudaMemsetAsync(c.out_velocities.p, 0, 12ull * n, c.stream), "memset");
+  check(cudaMemsetAsync(c.out_loads.p, 0, 4ull * n, c.stream), "memset");
+  check(cudaMemsetAsync(c.out_increments.p, 0, 4ull * n, c.stream), "memset");
+  if (dt == 0.0f) return out;
+  copy_geometry(c, c.initial, c.state);
+  copy_geometry(c, c.base, c.state);
+  c.has_memory = false;
+  c.memory.count = 0;
+
+  reset_scalars(c);
+  launch_growth_bound(n, c.state.view(), c.growth.p, dt, c.scalars.p + kGrowthBits, c.stream);
+  read_scalars(c);
+  const float growth = bits_to_float(c.host_scalars[kGrowthBits]);
+  const float pieces = std::max(1.0f, std::ceil(growth / p.max_growth_fraction));
+  if (!std::isfinite(pieces)) throw std::runtime_error("contact dynamics growth per step is not finite");
+  const float longest = dt / pieces;
+  const float shortest = std::ldexp(longest, -int(p.max_step_halvings));
+  double remaining = double(dt);
+  float length = longest;
+  float proven = 0.0f;
+  c.accepted_a.ensure(n);
+  c.accepted_b.ensure(n);
+  while (remaining > 0.0) {
+    if (double(length) >= remaining * (1.0 - 1.0e-6)) length = float(remaining);
+    const auto attempt = advance_substep(c, length, p, cp, wp, length > proven, out.report.iterations);
+    if (!attempt.accepted) {
+      const float excess = attempt.rotation / kPlannedSubstepRotation;
+      const std::uint32_t halvings = excess > 2.0f ? std::uint32_t(std::ceil(std::log2(excess))) : 1u;
+      const float failed = length;
+      length = std::ldexp(length, -int(std::min<std::uint32_t>(halvings, 64)));
+      out.report.halvings += halvings;
+      if (length < shortest) {
+        throw std::runtime_error("contact dynamics did not resolve the contacts of a substep of " +
+                                 std::to_string(failed));
+      }
+      continue;
+    }
+    remaining -= double(length);
+    proven = std::max(proven, length);
+    std::swap(c.base, c.trial);  // base <- the accepted trial geometry
+    check(cudaMemcpyAsync(c.accepted_a.p, c.resp_a.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, c.stream), "copy");
+    check(cudaMemcpyAsync(c.accepted_b.p, c.resp_b.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, c.stream), "copy");
+    ++out.report.substeps;
+    out.report.refinements += attempt.refinements;
+    out.report.max_rows = std::max<std::uint64_t>(out.report.max_rows, attempt.rows);
+    out.report.max_overlap = attempt.max_overlap;
+    std::swap(c.rows, c.memory);  // forces <- this substep's rows
+    c.has_memory = true;
+    if (attempt.refinements <= kEasyRefinements && 2.0f * attempt.rotation <= kPlannedSubstepRotation) {
+      length = std::min(longest, length * 2.0f);
+    }
+  }
+  launch_outputs(n, {c.accepted_a.p, c.accepted_b.p}, c.base.view(), c.initial.view(), c.out_velocities.p,
+                 c.out_loads.p, c.out_increments.p, c.stream);
+  return out;
+}
+
+void write_back(Ctx& c, msb_cell_arrays& cells, bool device_pointers) {
+  const std::size_t n = c.n;
+  if (n == 0) return;
+  launch_unpack_cells(c.n, c.state.view(), c.staging[0].p, c.staging[1].p, c.staging[2].p, c.staging[3].p,
+                      c.staging[4].p, c.staging[5].p, c.staging[6].p, c.stream);
+  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  float* dst[7] = {cells.position_x,  cells.position_y,  cells.position_z, cells.direction_x,
+                   cells.direction_y, cells.direction_z, cells.lengths};
+  for (int k = 0; k < 7; ++k) check(cudaMemcpyAsync(dst[k], c.staging[k].p, n * 4, kind, c.stream), "copy back");
+}
+
+void write_outputs(Ctx& c, msb_contact_dynamics_outputs* outputs, bool device_pointers) {
+  if (outputs == nullptr || c.n == 0) return;
+  const std::size_t n = c.n;
+  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  if (outputs->center_velocities != nullptr) {
+    check(cudaMemcpyAsync(outputs->center_velocities, c.out_velocities.p, 12 * n, kind, c.stream), "copy out");
+  }
+  if (outputs->axial_loads != nullptr) {
+    check(cudaMemcpyAsync(outputs->axial_loads, c.out_loads.p, 4 * n, kind, c.stream), "copy out");
+  }
+  if (outputs->length_increments != nullptr) {
+    check(cudaMemcpyAsync(outputs->length_increments, c.out_increments.p, 4 * n, kind, c.stream), "copy out");
+  }
+}
+
+// Uploads a ContactSystem's records as the context's rows and bodies.
+void load_system(Ctx& c, const msb_contact_system& s, const float* multipliers) {
+  validate_system(s);
+  c.n = std::uint32_t(s.body_count);
+  const std::uint32_t rows = std::uint32_t(s.row_count);
+  c.body_a.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.body_b.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.drift_a.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.drift_b.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.rows.ensure(std::max<std::uint32_t>(rows, 1));
+  c.rows.count = rows;
+  const std::size_t bytes = std::max<std::size_t>(rows * sizeof(msb_contact_row), c.n * sizeof(msb_contact_body));
+  c.records.ensure(std::max<std::size_t>(bytes, 1));
+  if (c.n > 0) {
+    check(cudaMemcpyAsync(c.records.p, s.bodies, c.n * sizeof(msb_contact_body), cudaMemcpyHostToDevice, c.stream),
+          "copy bodies");
+    launch_bodies_from_records(c.records.p, c.n, {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream);
+  }
+  if (rows > 0) {
+    check(cudaMemcpyAsync(c.records.p, s.rows, rows * sizeof(msb_contact_row), cudaMemcpyHostToDevice, c.stream),
+          "copy rows");
+    launch_rows_from_records(c.records.p, rows, c.rows.arrays(), c.stream);
+    check(cudaMemcpyAsync(c.rows.multipliers.p, multipliers, rows * 4ull, cudaMemcpyHostToDevice, c.stream),
+          "copy multipliers");
+  }
+  build_system_incidence(c, rows);
+}
+
+template <typename Body>
+int guarded(msb_context* c, Body&& body) {
+  if (c == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  try {
+    check(cudaSetDevice(c->device), "cudaSetDevice");
+    body();
+    c->error.clear();
+    return MSB_OK;
+  } catch (const std::invalid_argument& e) {
+    c->error = e.what();
+    return MSB_ERR_INVALID_ARGUMENT;
+  } catch (const std::overflow_error& e) {
+    c->error = e.what();
+    return MSB_ERR_OVERFLOW;
+  } catch (const CapacityError& e) {
+    c->error = e.what();
+    return MSB_ERR_CAPACITY;
+  } catch (const CudaError& e) {
+    c->error = e.what();
+    return MSB_ERR_CUDA;
+  } catch (const DeviceCheckError& e) {
+    c->error = e.what();
+    return MSB_ERR_DEVICE_CHECK;
+  } catch (const std::exception& e) {
+    c->error = e.what();
+    return MSB_ERR_RUNTIME;
+  }
+}
+
+}  // namespace
+}  // namespace msb
+
+using namespace msb;
+
+extern "C" {
+
+size_t msb_device_count(void) {
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  return std::size_t(count);
+}
+
+int msb_context_create(uint32_t device_index, msb_context** out) {
+  if (out == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  *out = nullptr;
+  int count = 0;
+  if (cudaGetDeviceCount(&count) != cudaSuccess || count == 0) {
+    cudaGetLastError();
+    return MSB_ERR_NO_DEVICE;
+  }
+  if (int(device_index) >= count) return MSB_ERR_INVALID_ARGUMENT;
+  auto context = std::make_unique<msb_context>();
+  context->device = int(device_index);
+  try {
+    check(cudaSetDevice(context->device), "cudaSetDevice");
+    cudaDeviceProp prop{};
+    check(cudaGetDeviceProperties(&prop, context->device), "properties");
+    context->device_name = prop.name;
+    check(cudaStreamCreateWithFlags(&context->stream, cudaStreamNonBlocking), "stream");
+    check(cudaMalloc(&context->desc, sizeof(SolveDesc)), "cudaMalloc");
+    check(cudaMemset(context->desc, 0, sizeof(SolveDesc)), "memset");
+    check(cudaMallocHost(&context->host_scalars, 2 * kScalarCount * sizeof(std::uint32_t)), "cudaMallocHost");
+    check(cudaMallocHost(&context->host_desc, sizeof(SolveDesc)), "cudaMallocHost");
+    std::memset(context->host_desc, 0, sizeof(SolveDesc));
+    context->scalars.ensure(kScalarCount);
+    check(cudaMemset(context->scalars.p, 0, kScalarCount * 4), "memset");
+  } catch (const std::exception& e) {
+    return MSB_ERR_CUDA;
+  }
+  context->launches_at_create = launches.load();
+  *out = context.release();
+  return MSB_OK;
+}
+
+void msb_context_destroy(msb_context* context) {
+  if (context == nullptr) return;
+  cudaSetDevice(context->device);
+  if (context->stream != nullptr) cudaStreamSynchronize(context->stream);
+  context->graphs.clear();
+  if (context->desc != nullptr) cudaFree(context->desc);
+  if (context->host_scalars != nullptr) cudaFreeHost(context->host_scalars);
+  if (context->host_desc != nullptr) cudaFreeHost(context->host_desc);
+  if (context->stream != nullptr) cudaStreamDestroy(context->stream);
+  delete context;
+}
+
+const char* msb_last_error(const msb_context* context) {
+  return context != nullptr ? context->error.c_str() : "no context";
+}
+
+int msb_backend_info(const msb_context* context, char* device_name, size_t capacity) {
+  if (context == nullptr || device_name == nullptr || capacity == 0) return MSB_ERR_INVALID_ARGUMENT;
+  std::snprintf(device_name, capacity, "%s", context->device_name.c_str());
+  return MSB_OK;
+}
+
+uint64_t msb_launch_count(const msb_context* context) {
+  return launches.load() - (context != nullptr ? context->launches_at_create : 0);
+}
+
+int msb_find_cell_contacts(msb_context* context, const msb_cell_arrays* cells,
+                           const msb_contact_parameters* parameters, msb_cell_contact* contacts, uint64_t capacity,
+                           uint64_t* count) {
+  return guarded(context, [&] {
+    if (cells == nullptr || parameters == nullptr || count == nullptr) throw std::invalid_argument("null argument");
+    validate_contact_parameters(*parameters);
+    auto& c = *context;
+    load_cells(c, *cells, false);
+    const ContactSearchParams prm{parameters->activation_margin, parameters->parallel_sine_threshold,
+                                  parameters->degeneracy_epsilon};
+    const std::uint32_t total = find_pairs(c, c.state, prm, c.touches);
+    *count = total;
+    if (total > capacity) throw CapacityError("contact array is too small");
+    if (total == 0) return;
+    if (contacts == nullptr) throw std::invalid_argument("null contact array");
+    c.records.ensure(total * sizeof(msb_cell_contact));
+    launch_touches_to_cell_contacts(c.touches.p, total, c.ids.p, c.records.p, c.stream);
+    check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_cell_contact), cudaMemcpyDeviceToHost, c.stream),
+          "copy contacts");
+    sync(c);
+  });
+}
+
+int msb_find_external_contacts(msb_context* context, const msb_cell_arrays* cells, const msb_constraint* constraints,
+                               uint64_t constraint_count, const msb_constraint_contact_parameters* parameters,
+                               uint32_t every_face, msb_external_contact* contacts, uint64_t capacity,
+                               uint64_t* count) {
+  return guarded(context, [&] {
+    if (cells == nullptr || parameters == nullptr || count == nullptr) throw std::invalid_argument("null argument");
+    validate_constraint_parameters(*parameters);
+    auto& c = *context;
+    load_cells(c, *cells, false);
+    load_constraints(c, constraints, constraint_count);
+    const std::uint32_t total =
+        find_walls(c, c.state, parameters->activation_margin, parameters->degeneracy_epsilon, every_face != 0,
+                   c.touches, 0);
+    *count = total;
+    if (total > capacity) throw CapacityError("contact array is too small");
+    if (total == 0) return;
+    if (contacts == nullptr) throw std::invalid_argument("null contact array");
+    c.records.ensure(total * sizeof(msb_external_contact));
+    launch_touches_to_external_contacts(c.touches.p, total, c.ids.p, c.records.p, c.stream);
+    check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_external_contact), cudaMemcpyDeviceToHost,
+                          c.stream),
+          "copy contacts");
+    sync(c);
+  });
+}
+
+int msb_solve_contact_forces(msb_context* context, const msb_contact_system* system, const float* initial,
+                             const msb_contact_solve_parameters* parameters, float* multipliers,
+                             msb_contact_solve_report* report) {
+  return guarded(context, [&] {
+    if (system == nullptr || parameters == nullptr || report == nullptr) throw std::invalid_argument("null argument");
+    if (system->row_count > 0 && (initial == nullptr || multipliers == nullptr || system->rows == nullptr)) {
+      throw std::invalid_argument("null row arrays");
+    }
+    if (system->body_count > 0 && system->bodies == nullptr) throw std::invalid_argument("null body array");
+    validate_system(*system);
+    require_multipliers(initial, system->row_count);
+    if (!std::isfinite(parameters->tolerance) || parameters->tolerance <= 0.0f) {
+      throw std::invalid_argument("contact solve tolerance must be finite and positive");
+    }
+    *report = {MSB_SOLVE_CONVERGED, 0, 0.0f};
+    if (system->row_count == 0) return;
+    auto& c = *context;
+    load_system(c, *system, initial);
+    const auto outcome = solve(c, system->dt, system->growth, parameters->tolerance, parameters->max_iterations);
+    check(cudaMemcpyAsync(multipliers, c.rows.multipliers.p, system->row_count * 4, cudaMemcpyDeviceToHost, c.stream),
+          "copy multipliers");
+    sync(c);
+    *report = {outcome.status, outcome.iterations, outcome.residual};
+  });
+}
+
+int msb_evaluate_contact_response(msb_context* context, const msb_contact_system* system, const float* multipliers,
+                                  float* velocities, float* loads, float* length_rates) {
+  return guarded(context, [&] {
+    if (system == nullptr) throw std::invalid_argument("null argument");
+    validate_system(*system);
+    if (system->row_count > 0) {
+      if (multipliers == nullptr) throw std::invalid_argument("null multipliers");
+      require_multipliers(multipliers, system->row_count);
+    }
+    auto& c = *context;
+    load_system(c, *system, multipliers);
+    c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
+    c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
+    fill_desc(c, c.rows.count, system->dt, system->growth, 1.0f, 0);
+    launch_evaluate(c.desc, std::max(1, grid_for(std::max<std::uint32_t>(c.n, 1), kSolveThreads)), false, c.stream);
+    if (c.n == 0) return;
+    c.out_velocities.ensure(6ull * c.n);
+    c.out_loads.ensure(c.n);
+    c.out_increments.ensure(c.n);
+    launch_response_to_host_layout(c.n, {c.resp_a.p, c.resp_b.p}, c.out_velocities.p, c.out_loads.p,
+                                   c.out_increments.p, c.stream);
+    if (velocities) check(cudaMemcpyAsync(velocities, c.out_velocities.p, 24ull * c.n, cudaMemcpyDeviceToHost, c.stream), "copy");
+    if (loads) check(cudaMemcpyAsync(loads, c.out_loads.p, 4ull * c.n, cudaMemcpyDeviceToHost, c.stream), "copy");
+    if (length_rates) check(cudaMemcpyAsync(length_rates, c.out_increments.p, 4ull * c.n, cudaMemcpyDeviceToHost, c.stream), "copy");
+    sync(c);
+  });
+}
+
+int msb_evaluate_contact_gaps(msb_context* context, const msb_contact_system* system, const float* multipliers,
+                              float* gaps) {
+  return guarded(context, [&] {
+    if (system == nullptr) throw std::invalid_argument("null argument");
+    validate_system(*system);
+    if (system->row_count == 0) return;
+    if (multipliers == nullptr || gaps == nullptr) throw std::invalid_argument("null arrays");
+    require_multipliers(multipliers, system->row_count);
+    auto& c = *context;
+    load_system(c, *system, multipliers);
+    c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
+    c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
+    fill_desc(c, c.rows.count, system->dt, system->growth, 1.0f, 0);
+    launch_evaluate(c.desc, std::max(1, grid_for(std::max(c.rows.count, c.n), kSolveThreads)), true, c.stream);
+    check(cudaMemcpyAsync(gaps, c.rows.gaps.p, system->row_count * 4, cudaMemcpyDeviceToHost, c.stream), "copy");
+    sync(c);
+  });
+}
+
+int msb_contact_system_diagonal_bound(msb_context* context, const msb_contact_system* system, float* bound) {
+  return guarded(context, [&] {
+    if (system == nullptr || bound == nullptr) throw std::invalid_argument("null argument");
+    validate_system(*system);
+    *bound = 0.0f;
+    if (system->row_count == 0) return;
+    auto& c = *context;
+    std::vector<float> zeros(system->row_count, 0.0f);
+    load_system(c, *system, zeros.data());
+    // A solve capped at zero iterations computes the bound and stops.
+    c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
+    c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
+    auto& graph = graph_for(c, std::max(c.rows.count, c.n));
+    c.partials.ensure(5ull * 1184);
+    fill_desc(c, c.rows.count, system->dt, system->growth, 1.0f, 0);
+    check(cudaError_t(graph.launch(c.stream)), "launch");
+    check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read");
+    sync(c);
+    *bound = c.host_desc->bound;
+  });
+}
+
+int msb_profile_iterations(msb_context* context, uint32_t iterations, float* body_ms, float* row_ms,
+                           uint64_t* rows, uint64_t* bodies) {
+  return guarded(context, [&] {
+    auto& c = *context;
+    if (c.last_blocks == 0 || iterations == 0) throw std::invalid_argument("no solved system to time");
+    cudaEvent_t start, between, stop;
+    check(cudaEventCreate(&start), "event");
+    check(cudaEventCreate(&between), "event");
+    check(cudaEventCreate(&stop), "event");
+    // Warm the caches as the solve loop does.
+    launch_iteration(c.desc, c.last_blocks, nullptr, c.stream);
+    double body = 0.0, row = 0.0;
+    for (std::uint32_t k = 0; k < iterations; ++k) {
+      check(cudaEventRecord(start, c.stream), "event");
+      launch_iteration(c.desc, c.last_blocks, between, c.stream);
+      check(cudaEventRecord(stop, c.stream), "event");
+      check(cudaEventSynchronize(stop), "event");
+      float a = 0.0f, b = 0.0f;
+      check(cudaEventElapsedTime(&a, start, between), "event");
+      check(cudaEventElapsedTime(&b, between, stop), "event");
+      body += a;
+      row += b;
+    }
+    cudaEventDestroy(start);
+    cudaEventDestroy(between);
+    cudaEventDestroy(stop);
+    check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read");
+    sync(c);
+    *body_ms = float(body / iterations);
+    *row_ms = float(row / iterations);
+    *rows = c.host_desc->row_count;
+    *bodies = c.host_desc->body_count;
+  });
+}
+
+static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb_constraint* constraints,
+                         uint64_t constraint_count, float dt, const msb_contact_dynamics_parameters* dynamics,
+                         const msb_contact_parameters* contacts,
+                         const msb_constraint_contact_parameters* constraint_parameters,
+                         msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs,
+                         bool device_pointers) {
+  return guarded(context, [&] {
+    if (cells == nullptr || dynamics == nullptr || report == nullptr) throw std::invalid_argument("null argument");
+    if (!std::isfinite(dt) || dt < 0.0f) throw std::invalid_argument("time step must be finite and non-negative");
+    const msb_contact_parameters cp = contacts != nullptr ? *contacts : msb_contact_parameters{0.01f, 0.1f, 1.0e-6f};
+    const msb_constraint_contact_parameters wp =
+        constraint_parameters != nullptr ? *constraint_parameters : msb_constraint_contact_parameters{0.0f, 1.0e-6f};
+    validate_dynamics(*dynamics);
+    validate_contact_parameters(cp);
+    validate_constraint_parameters(wp);
+    auto& c = *context;
+    load_cells(c, *cells, device_pointers);
+    load_constraints(c, constraints, constraint_count);
+    const auto outcome = advance(c, dt, *dynamics, cp, wp);
+    write_back(c, *cells, device_pointers);
+    write_outputs(c, outputs, device_pointers);
+    sync(c);
+    *report = outcome.report;
+  });
+}
+
+int msb_advance_contact_dynamics(msb_context* context, msb_cell_arrays* cells, const msb_constraint* constraints,
+                                 uint64_t constraint_count, float dt, const msb_contact_dynamics_parameters* dynamics,
+                                 const msb_contact_parameters* contacts,
+                                 const msb_constraint_contact_parameters* constraint_parameters,
+                                 msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs) {
+  return advance_entry(context, cells, constraints, constraint_count, dt, dynamics, contacts, constraint_parameters,
+                       report, outputs, false);
+}
+
+int msb_advance_contact_dynamics_device(msb_context* context, msb_cell_arrays* cells,
+                                        const msb_constraint* constraints, uint64_t constraint_count, float dt,
+                                        const msb_contact_dynamics_parameters* dynamics,
+                                        const msb_contact_parameters* contacts,
+                                        const msb_constraint_contact_parameters* constraint_parameters,
+                                        msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs) {
+  return advance_entry(context, cells, constraints, constraint_count, dt, dynamics, contacts, constraint_parameters,
+                       report, outputs, true);
+}
+
+}  // extern "C"

@@ -1,0 +1,470 @@
+// Barzilai-Borwein projected gradient on the contact multipliers, resident on
+// the device (cpp/core/contact_solver.hpp:44-120,
+// cpp/cpu/cpu_contact_dynamics.cpp:40-338 of the reference).
+//
+// One iteration is two passes:
+//   body pass  one thread per body sums its rows' projected multipliers
+//              times their jacobians in row order (the reference's
+//              incidence order, so a body's force and torque carry the same
+//              bits), then applies the mobility and the growth-load law;
+//   row pass   one thread per row forms the new gap, the FP64 BB products
+//              and the complementarity residual; the last block to finish
+//              combines the per-block partials in block order (so the result
+//              does not depend on scheduling), sets the next step length and
+//              the convergence flag, and writes the flag into the WHILE node
+//              of the CUDA graph that repeats the two passes.
+// The host launches the graph once per solve and reads the report once.
+
+#include <cfloat>
+#include <cstdint>
+
+#include "device.cuh"
+#include "kernels.h"
+#include "solve.h"
+#include "../../include/msb200.h"
+
+namespace msb {
+namespace {
+
+__device__ __forceinline__ float growth_factor(std::uint32_t law, float sensitivity, float free_load,
+                                               float stall_load, float load) {
+  if (law == MSB_GROWTH_LAW_EXPONENTIAL) {
+    // exp in FP64 rounded once to FP32.
+    return float(exp(double(-sensitivity * smax(0.0f, load))));
+  }
+  if (law == MSB_GROWTH_LAW_LINEAR) {
+    return sclamp(1.0f - (load - free_load) / (stall_load - free_load), 0.0f, 1.0f);
+  }
+  return 1.0f;
+}
+
+// apply_mobility (cpu_contact_dynamics.cpp:40-53) plus drift.
+__device__ __forceinline__ void respond(const SolveDesc& d, std::uint32_t b, const float w[6], float load) {
+  const float4 ba = d.bodies.a[b];
+  const float4 bb = d.bodies.b[b];
+  const float4 da = d.bodies.drift_a[b];
+  const float4 db = d.bodies.drift_b[b];
+  const F3 axis{ba.x, ba.y, ba.z};
+  const F3 tq{w[3], w[4], w[5]};
+  const float s = (bb.y - bb.x) * dot(axis, tq);
+  const F3 ang = tq * bb.x + axis * s;
+  float v[6] = {w[0] * ba.w, w[1] * ba.w, w[2] * ba.w, ang.x, ang.y, ang.z};
+  v[0] += da.x;
+  v[1] += da.y;
+  v[2] += da.z;
+  v[3] += db.x;
+  v[4] += db.y;
+  v[5] += db.z;
+  const float rate = bb.z > 0.0f ? bb.z * growth_factor(d.law, d.sensitivity, d.free_load, d.stall_load, load) : bb.z;
+  d.response.a[b] = make_float4(v[0], v[1], v[2], rate);
+  d.response.b[b] = make_float4(v[3], v[4], v[5], load);
+}
+
+// mode 0 and 2 evaluate the multipliers as they are; mode 1 their projection.
+__global__ void __launch_bounds__(kSolveThreads) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
+  const SolveDesc& d = *desc;
+  const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
+  const float alpha = d.step;
+  const float* __restrict__ g = d.multipliers;
+  const float* __restrict__ gap = d.gaps;
+  for (std::uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < d.body_count; b += gridDim.x * blockDim.x) {
+    float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    float load = 0.0f;
+    const std::uint32_t end = d.incidence.offsets[b + 1];
+    for (std::uint32_t k = d.incidence.offsets[b]; k < end; ++k) {
+      const float4 ea = d.incidence.a[k];
+      const float4 eb = d.incidence.b[k];
+      const std::uint32_t row = __float_as_uint(eb.w);
+      const float m = mode == 1 ? smax(0.0f, g[row] - alpha * gap[row]) : g[row];
+      if (m == 0.0f) continue;
+      w[0] += m * ea.x;
+      w[1] += m * ea.y;
+      w[2] += m * ea.z;
+      w[3] += m * ea.w;
+      w[4] += m * eb.x;
+      w[5] += m * eb.y;
+      load += eb.z * m;
+    }
+    respond(d, b, w, load);
+  }
+}
+
+__device__ __forceinline__ float wrench_dot(float4 ja, float4 jb, float4 va, float4 vb) {
+  float r = 0.0f;
+  r += ja.x * va.x;
+  r += ja.y * va.y;
+  r += ja.z * va.z;
+  r += ja.w * vb.x;
+  r += jb.x * vb.y;
+  r += jb.y * vb.z;
+  return r;
+}
+
+__device__ __forceinline__ float row_residual(float m, float gap) {
+  return m > 0.0f ? fabsf(gap) : smax(0.0f, -gap);
+}
+
+// next_contact_step_length (contact_solver.hpp:54-62).
+__device__ __forceinline__ float next_step(float current, double ss, double sy, double yy, std::uint32_t iteration) {
+  if (!(sy > 0.0) || !(yy > 0.0)) return current;
+  const double next = (iteration % 2u) == 1u ? ss / sy : sy / yy;
+  return isfinite(next) && next > 0.0 ? float(next) : current;
+}
+
+// mode 0: gaps of the initial multipliers and the first residual (sets the
+// graph condition); mode 1: one projected step (sets the condition);
+// mode 2: gaps only.
+__global__ void __launch_bounds__(kSolveThreads) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
+  SolveDesc& d = *desc;
+  const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
+  const float alpha = d.step;
+  const float dt = d.dt;
+  float* __restrict__ g = d.multipliers;
+  float* __restrict__ gap = d.gaps;
+  double ss = 0.0, sy = 0.0, yy = 0.0;
+  float residual = 0.0f;
+  bool finite = true;
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    const float gpi = mode == 1 ? gap[i] : 0.0f;
+    const float m = mode == 1 ? smax(0.0f, gi - alpha * gpi) : gi;
+    const uint2 s = d.rows.slots[i];
+    const float4 ra = d.rows.a[i];
+    const float4 rb = d.rows.b[i];
+    const float4 va = d.response.a[s.x];
+    const float4 vb = d.response.b[s.x];
+    float rate = wrench_dot(ra, rb, va, vb) - rb.z * va.w;
+    float4 rd = d.rows.d[i];
+    if (s.y != kInvalidSlot) {
+      const float4 rc = d.rows.c[i];
+      const float4 wa = d.response.a[s.y];
+      const float4 wb = d.response.b[s.y];
+      rate += wrench_dot(rc, rd, wa, wb) - rd.z * wa.w;
+    }
+    const float gn = rb.w + dt * rate + rd.w * m;
+    residual = smax(residual, row_residual(m, gn));
+    finite = finite && isfinite(gn);
+    if (mode == 1) {
+      const double moved = double(m) - double(gi);
+      const double change = double(gn) - double(gpi);
+      ss += moved * moved;
+      sy += moved * change;
+      yy += change * change;
+      g[i] = m;
+    }
+    gap[i] = gn;
+  }
+  if (mode == 2) return;
+
+  // Block reduction in a fixed tree.
+  __shared__ double red[5][kSolveThreads / 32];
+  double v[5] = {ss, sy, yy, double(residual), finite ? 1.0 : 0.0};
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_down_sync(0xFFFFFFFFu, v[k], o);
+      v[k] = k < 3 ? v[k] + other : (k == 3 ? fmax(v[k], other) : fmin(v[k], other));
+    }
+    if (lane == 0) red[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x < 5) {
+    const int k = threadIdx.x;
+    double r = red[k][0];
+    for (int w = 1; w < kSolveThreads / 32; ++w) {
+      r = k < 3 ? r + red[k][w] : (k == 3 ? fmax(r, red[k][w]) : fmin(r, red[k][w]));
+    }
+    d.partials[5 * blockIdx.x + k] = r;
+  }
+  __threadfence();
+  __syncthreads();
+  __shared__ bool last;
+  if (threadIdx.x == 0) last = atomicAdd(&d.ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+
+  // The last block: combine the partials of every block in block order.
+  __threadfence();
+  double t[5] = {0.0, 0.0, 0.0, 0.0, 1.0};
+  for (std::uint32_t p = threadIdx.x; p < gridDim.x; p += blockDim.x) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) {
+      const double x = __ldcg(&d.partials[5 * p + k]);
+      t[k] = k < 3 ? t[k] + x : (k == 3 ? fmax(t[k], x) : fmin(t[k], x));
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_down_sync(0xFFFFFFFFu, t[k], o);
+      t[k] = k < 3 ? t[k] + other : (k == 3 ? fmax(t[k], other) : fmin(t[k], other));
+    }
+  }
+  __syncthreads();
+  if (lane == 0) {
+#pragma unroll
+    for (int k = 0; k < 5; ++k) red[k][warp] = t[k];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  double total[5];
+  for (int k = 0; k < 5; ++k) {
+    total[k] = red[k][0];
+    for (int w = 1; w < kSolveThreads / 32; ++w) {
+      total[k] = k < 3 ? total[k] + red[k][w] : (k == 3 ? fmax(total[k], red[k][w]) : fmin(total[k], red[k][w]));
+    }
+  }
+  d.ticket = 0;
+  const float reported = total[4] > 0.5 ? float(total[3]) : __int_as_float(0x7FC00000);
+  d.residual = reported;
+  std::uint32_t proceed = 0;
+  if (mode == 0) {
+    const float bound = __uint_as_float(d.bound_bits);
+    d.bound = bound;
+    d.iterations = 0;
+    if (!isfinite(bound) || !(bound > 0.0f)) {
+      d.status = 3;  // no positive diagonal: an invalid system
+    } else if (!isfinite(reported)) {
+      d.status = MSB_SOLVE_BREAKDOWN;
+    } else if (reported <= d.tolerance) {
+      d.status = MSB_SOLVE_CONVERGED;
+    } else {
+      d.status = MSB_SOLVE_ITERATION_LIMIT;
+      d.step = 1.0f / bound;
+      proceed = d.max_iterations > 0 ? 1u : 0u;
+    }
+    d.mode = 1;
+  } else {
+    const std::uint32_t iteration = d.iterations + 1;
+    d.iterations = iteration;
+    if (!isfinite(reported)) {
+      d.status = MSB_SOLVE_BREAKDOWN;
+    } else if (!(reported > d.tolerance)) {
+      d.status = MSB_SOLVE_CONVERGED;
+    } else {
+      d.step = next_step(d.step, total[0], total[1], total[2], iteration);
+      d.status = MSB_SOLVE_ITERATION_LIMIT;
+      proceed = iteration < d.max_iterations ? 1u : 0u;
+    }
+  }
+  d.proceed = proceed;
+  if (set_condition) cudaGraphSetConditional(cudaGraphConditionalHandle(d.handle), proceed);
+}
+
+// contact_system_diagonal_bound (cpu_contact_dynamics.cpp:247-260).
+__device__ __forceinline__ float diagonal(float4 ja, float4 jb, float4 ba, float4 bb) {
+  const F3 axis{ba.x, ba.y, ba.z};
+  const F3 tq{ja.w, jb.x, jb.y};
+  const float s = (bb.y - bb.x) * dot(axis, tq);
+  const F3 ang = tq * bb.x + axis * s;
+  float r = 0.0f;
+  r += ja.x * (ja.x * ba.w);
+  r += ja.y * (ja.y * ba.w);
+  r += ja.z * (ja.z * ba.w);
+  r += ja.w * ang.x;
+  r += jb.x * ang.y;
+  r += jb.y * ang.z;
+  return r;
+}
+
+__global__ void __launch_bounds__(kSolveThreads) bound_kernel(SolveDesc* desc) {
+  SolveDesc& d = *desc;
+  float bound = 0.0f;
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
+    const uint2 s = d.rows.slots[i];
+    const float4 ra = d.rows.a[i];
+    const float4 rb = d.rows.b[i];
+    float entry = diagonal(ra, rb, d.bodies.a[s.x], d.bodies.b[s.x]);
+    const float4 rd = d.rows.d[i];
+    if (s.y != kInvalidSlot) entry += diagonal(d.rows.c[i], rd, d.bodies.a[s.y], d.bodies.b[s.y]);
+    bound = smax(bound, d.dt * entry + rd.w);
+  }
+  for (int o = 16; o > 0; o >>= 1) bound = smax(bound, __shfl_down_sync(0xFFFFFFFFu, bound, o));
+  // Non-negative floats order as their bit patterns.
+  if ((threadIdx.x & 31) == 0 && bound > 0.0f) atomicMax(&d.bound_bits, __float_as_uint(bound));
+}
+
+__global__ void solve_reset_kernel(SolveDesc* desc) {
+  if (threadIdx.x == 0) {
+    desc->mode = 0;
+    desc->ticket = 0;
+    desc->iterations = 0;
+    desc->bound_bits = 0;
+    desc->status = MSB_SOLVE_CONVERGED;
+    desc->proceed = 0;
+  }
+}
+
+// ------------------------------------------------------------- incidence
+
+__global__ void incidence_keys_kernel(const uint2* __restrict__ slots, std::uint32_t rows, std::uint32_t bodies,
+                                      std::uint32_t* __restrict__ keys, std::uint32_t* __restrict__ values,
+                                      std::uint32_t* __restrict__ counts) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const uint2 s = slots[i];
+    keys[2 * std::uint64_t(i)] = s.x;
+    values[2 * std::uint64_t(i)] = i << 1;
+    atomicAdd(&counts[s.x], 1u);
+    if (s.y != kInvalidSlot) {
+      keys[2 * std::uint64_t(i) + 1] = s.y;
+      atomicAdd(&counts[s.y], 1u);
+    } else {
+      keys[2 * std::uint64_t(i) + 1] = bodies;  // sorts past every body
+    }
+    values[2 * std::uint64_t(i) + 1] = (i << 1) | 1u;
+  }
+}
+
+__global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __restrict__ values, std::uint32_t entries,
+                                        float4* __restrict__ out_a, float4* __restrict__ out_b) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < entries; k += gridDim.x * blockDim.x) {
+    const std::uint32_t v = values[k];
+    const std::uint32_t row = v >> 1;
+    if (v & 1u) {
+      const float4 c = r.c[row];
+      const float4 d = r.d[row];
+      out_a[k] = c;
+      out_b[k] = make_float4(d.x, d.y, d.z, __uint_as_float(row));
+    } else {
+      const float4 a = r.a[row];
+      const float4 b = r.b[row];
+      out_a[k] = a;
+      out_b[k] = make_float4(b.x, b.y, b.z, __uint_as_float(row));
+    }
+  }
+}
+
+__global__ void keyed_keys_kernel(const uint2* __restrict__ slots, std::uint32_t rows, std::uint32_t* __restrict__ keys,
+                                  std::uint32_t* __restrict__ values, std::uint32_t* __restrict__ counts) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const std::uint32_t s = slots[i].x;
+    keys[i] = s;
+    values[i] = i;
+    atomicAdd(&counts[s], 1u);
+  }
+}
+
+int bits_for(std::uint32_t value) {
+  int bits = 0;
+  while (bits < 32 && (std::uint64_t(1) << bits) <= value) ++bits;
+  return bits;
+}
+
+}  // namespace
+
+void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
+                     std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
+                     cudaStream_t stream) {
+  cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
+  if (row_count > 0) {
+    incidence_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, body_count, keys,
+                                                                          values, counts);
+    count_launch();
+  }
+  exclusive_scan(counts, incidence.offsets, body_count + 1, temp, stream);
+  if (row_count == 0) return;
+  const std::uint64_t n = 2ull * row_count;
+  radix_sort_pairs(keys, values, n, bits_for(body_count), temp, stream);
+  // Wall rows have no second entry; those sorted to the end and are dropped
+  // by gathering only as many entries as the offsets count (read on device
+  // through the last offset would need a sync, so gather all 2R and let the
+  // offsets bound what the body pass reads).
+  incidence_gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(rows, values, std::uint32_t(n), incidence.a,
+                                                                 incidence.b);
+  count_launch();
+}
+
+void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,
+                 std::uint32_t* rows_out, std::uint32_t* keys, std::uint32_t* counts, std::uint32_t* temp,
+                 cudaStream_t stream) {
+  cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
+  if (row_count > 0) {
+    keyed_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(slots, row_count, keys, rows_out, counts);
+    count_launch();
+  }
+  exclusive_scan(counts, offsets, body_count + 1, temp, stream);
+  if (row_count > 1) radix_sort_pairs(keys, rows_out, row_count, bits_for(body_count - 1), temp, stream);
+}
+
+SolveGraph::~SolveGraph() {
+  if (exec_ != nullptr) cudaGraphExecDestroy(exec_);
+  if (graph_ != nullptr) cudaGraphDestroy(graph_);
+}
+
+int SolveGraph::create(SolveDesc* desc, int blocks, cudaStream_t stream) {
+  blocks_ = blocks;
+  desc_ = desc;
+  cudaError_t err = cudaGraphCreate(&graph_, 0);
+  if (err != cudaSuccess) return err;
+  cudaGraphConditionalHandle handle;
+  err = cudaGraphConditionalHandleCreate(&handle, graph_, 0, cudaGraphCondAssignDefault);
+  if (err != cudaSuccess) return err;
+  handle_ = handle;
+
+  auto kernel_node = [&](cudaGraph_t graph, cudaGraphNode_t* node, const cudaGraphNode_t* deps, size_t ndeps,
+                         void* func, void** args, int grid, int threads = kSolveThreads) {
+    cudaKernelNodeParams p{};
+    p.func = func;
+    p.gridDim = dim3(grid);
+    p.blockDim = dim3(threads);
+    p.sharedMemBytes = 0;
+    p.kernelParams = args;
+    p.extra = nullptr;
+    return cudaGraphAddKernelNode(node, graph, deps, ndeps, &p);
+  };
+
+  SolveDesc* d = desc;
+  int mode_auto = -1;
+  int with_condition = 1;
+  void* reset_args[] = {&d};
+  void* bound_args[] = {&d};
+  void* body_args[] = {&d, &mode_auto};
+  void* row_args[] = {&d, &mode_auto, &with_condition};
+  cudaGraphNode_t reset, bound, body0, row0, loop;
+  if ((err = kernel_node(graph_, &reset, nullptr, 0, (void*)solve_reset_kernel, reset_args, 1, 32)) != cudaSuccess) return err;
+  if ((err = kernel_node(graph_, &bound, &reset, 1, (void*)bound_kernel, bound_args, blocks)) != cudaSuccess) return err;
+  if ((err = kernel_node(graph_, &body0, &bound, 1, (void*)body_pass_kernel, body_args, blocks)) != cudaSuccess) return err;
+  if ((err = kernel_node(graph_, &row0, &body0, 1, (void*)row_pass_kernel, row_args, blocks)) != cudaSuccess) return err;
+
+  cudaGraphNodeParams cp{};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = handle;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  if ((err = cudaGraphAddNode(&loop, graph_, &row0, 1, &cp)) != cudaSuccess) return err;
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  cudaGraphNode_t body1, row1;
+  if ((err = kernel_node(body, &body1, nullptr, 0, (void*)body_pass_kernel, body_args, blocks)) != cudaSuccess) return err;
+  if ((err = kernel_node(body, &row1, &body1, 1, (void*)row_pass_kernel, row_args, blocks)) != cudaSuccess) return err;
+  err = cudaGraphInstantiate(&exec_, graph_, 0);
+  count_launch(0);
+  return err;
+}
+
+int SolveGraph::launch(cudaStream_t stream) {
+  // Each graph has its own WHILE-node handle; the row pass reads it here.
+  cudaError_t err = cudaMemcpyAsync(&desc_->handle, &handle_, sizeof(handle_), cudaMemcpyHostToDevice, stream);
+  if (err != cudaSuccess) return err;
+  count_launch(4);
+  return cudaGraphLaunch(exec_, stream);
+}
+
+void launch_iteration(SolveDesc* desc, int blocks, cudaEvent_t between, cudaStream_t stream) {
+  body_pass_kernel<<<blocks, kSolveThreads, 0, stream>>>(desc, 1);
+  if (between != nullptr) cudaEventRecord(between, stream);
+  row_pass_kernel<<<blocks, kSolveThreads, 0, stream>>>(desc, 1, 0);
+  count_launch(2);
+}
+
+void launch_evaluate(SolveDesc* desc, int blocks, bool with_gaps, cudaStream_t stream) {
+  body_pass_kernel<<<blocks, kSolveThreads, 0, stream>>>(desc, 2);
+  count_launch();
+  if (with_gaps) {
+    row_pass_kernel<<<blocks, kSolveThreads, 0, stream>>>(desc, 2, 0);
+    count_launch();
+  }
+}
+
+}  // namespace msb

@@ -1,0 +1,487 @@
+// Per-cell and per-row passes of the contact stepper
+// (cpp/core/contact_dynamics.cpp:215-582 of the reference), in FP32 with the
+// reference's operation order.
+
+#include <cfloat>
+#include <cstdint>
+
+#include "device.cuh"
+#include "kernels.h"
+#include "step.h"
+#include "../../include/msb200.h"
+
+namespace msb {
+namespace {
+
+constexpr int kThreads = 256;
+constexpr float kMaximumSubstepRotation = 0.5f;
+constexpr float kMinimumLeverLength = 1.0e-6f;
+
+__device__ __forceinline__ void atomic_max_nonnegative(std::uint32_t* bits, float value) {
+  if (value > 0.0f) atomicMax(bits, __float_as_uint(value));
+}
+
+__global__ void pack_cells_kernel(std::uint32_t n, const float* px, const float* py, const float* pz,
+                                  const float* dx, const float* dy, const float* dz, const float* len,
+                                  const float* radius, GeometryBuffers out, std::uint32_t* status) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const F3 p{px[i], py[i], pz[i]};
+    const F3 d{dx[i], dy[i], dz[i]};
+    const float l = len[i];
+    const float r = radius[i];
+    const float m = norm(d);
+    if (!finite3(p) || !finite3(d) || !isfinite(l) || !isfinite(r) || l < 0.0f || !(r > 0.0f) ||
+        !(fabsf(m - 1.0f) <= 1.0e-5f)) {
+      raise_status(status, kStatusGeometry);
+    }
+    out.pos_len[i] = make_float4(p.x, p.y, p.z, l);
+    out.dir_rad[i] = make_float4(d.x, d.y, d.z, r);
+  }
+}
+
+__global__ void unpack_cells_kernel(std::uint32_t n, GeometryBuffers in, float* px, float* py, float* pz, float* dx,
+                                    float* dy, float* dz, float* len) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const float4 pl = in.pos_len[i];
+    const float4 dr = in.dir_rad[i];
+    px[i] = pl.x;
+    py[i] = pl.y;
+    pz[i] = pl.z;
+    len[i] = pl.w;
+    dx[i] = dr.x;
+    dy[i] = dr.y;
+    dz[i] = dr.z;
+  }
+}
+
+__global__ void make_bodies_kernel(std::uint32_t n, GeometryBuffers state, const float* __restrict__ growth,
+                                   const std::uint8_t* __restrict__ fixed, GeometryBuffers rate_lengths,
+                                   float drag, BodyArrays bodies) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 pl = state.pos_len[s];
+    const float4 dr = state.dir_rad[s];
+    const float rate = growth[s] * rate_lengths.pos_len[s].w;
+    float mt = 0.0f, ma = 0.0f, mtr = 0.0f;
+    if (fixed == nullptr || fixed[s] == 0) {
+      const float r = dr.w;
+      const float total = pl.w + 2.0f * r;
+      const float tr = drag * total;
+      const float ax = 0.5f * tr * r * r;
+      const float tv = tr * ((total * total) + 3.0f * r * r) / 12.0f;
+      mt = 1.0f / tr;
+      ma = 1.0f / ax;
+      mtr = 1.0f / tv;
+    }
+    bodies.a[s] = make_float4(dr.x, dr.y, dr.z, mt);
+    bodies.b[s] = make_float4(mtr, ma, rate, 0.0f);
+    bodies.drift_a[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    bodies.drift_b[s] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+}
+
+// length_lever (contact_dynamics.cpp:215-224).
+__device__ __forceinline__ float length_lever(float4 pl, float4 dr, F3 centre, F3 outward) {
+  const float length = pl.w;
+  if (length <= kMinimumLeverLength) return 0.0f;
+  const F3 axis = xyz(dr);
+  const float coordinate = dot(axis, centre - xyz(pl)) / length;
+  return smax(0.0f, sclamp(coordinate, -0.5f, 0.5f) * dot(axis, outward));
+}
+
+__device__ __forceinline__ float wrench_dot(float4 ja, float4 jb, float4 va, float4 vb) {
+  float r = 0.0f;
+  r += ja.x * va.x;
+  r += ja.y * va.y;
+  r += ja.z * va.z;
+  r += ja.w * vb.x;
+  r += jb.x * vb.y;
+  r += jb.y * vb.z;
+  return r;
+}
+
+__global__ void make_rows_kernel(const Touch* __restrict__ touches, std::uint32_t count, GeometryBuffers geometry,
+                                 RowBuild prm, ResponseArrays response, int correct, RowArrays rows,
+                                 std::uint32_t row_base, std::uint64_t* __restrict__ key_partner,
+                                 float* __restrict__ multipliers, std::uint32_t* overlap_bits) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const Touch t = touches[k];
+    const bool wall = t.s2 == kInvalidSlot;
+    const float compliance = 1.0f / (wall ? prm.wall_stiffness : prm.contact_stiffness);
+    float offset = smax(t.sep, -prm.recovery);
+    const float c = t.sep < -prm.recovery ? compliance * prm.recovery / -t.sep : compliance;
+    const F3 n{t.normal[0], t.normal[1], t.normal[2]};
+    const F3 p{t.point[0], t.point[1], t.point[2]};
+    const float4 pl1 = geometry.pos_len[t.s1];
+    const float4 dr1 = geometry.dir_rad[t.s1];
+    const F3 a1 = cross(p - xyz(pl1), n);
+    const float l1 = length_lever(pl1, dr1, p - n * dr1.w, n);
+    float4 ra = make_float4(-n.x, -n.y, -n.z, -a1.x);
+    float4 rb = make_float4(-a1.y, -a1.z, l1, offset);
+    float4 rc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 rd = make_float4(0.0f, 0.0f, 0.0f, c);
+    if (!wall) {
+      const float4 pl2 = geometry.pos_len[t.s2];
+      const float4 dr2 = geometry.dir_rad[t.s2];
+      const F3 a2 = cross(p - xyz(pl2), n);
+      const float l2 = length_lever(pl2, dr2, p + n * (t.sep + dr2.w), n * -1.0f);
+      rc = make_float4(n.x, n.y, n.z, a2.x);
+      rd = make_float4(a2.y, a2.z, l2, c);
+    }
+    if (correct) {
+      // predicted_rate (contact_dynamics.cpp:286-301)
+      float rate = wrench_dot(ra, rb, response.a[t.s1], response.b[t.s1]) - rb.z * response.a[t.s1].w;
+      if (!wall) rate += wrench_dot(rc, rd, response.a[t.s2], response.b[t.s2]) - rd.z * response.a[t.s2].w;
+      offset -= prm.dt * rate;
+      rb.w = offset;
+    }
+    const std::uint32_t i = row_base + k;
+    rows.a[i] = ra;
+    rows.b[i] = rb;
+    rows.c[i] = rc;
+    rows.d[i] = rd;
+    rows.slots[i] = make_uint2(t.s1, t.s2);
+    key_partner[i] = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
+    multipliers[i] = 0.0f;
+    atomic_max_nonnegative(overlap_bits, -t.sep);
+  }
+}
+
+__global__ void warm_start_kernel(std::uint32_t rows, const uint2* __restrict__ slots, KeyedLists current,
+                                  KeyedLists memory, int has_memory, float* __restrict__ multipliers) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const std::uint32_t first = slots[i].x;
+    const std::uint64_t key = current.partner[i];
+    std::uint32_t occurrence = 0;
+    for (std::uint32_t k = current.offsets[first]; k < current.offsets[first + 1]; ++k) {
+      const std::uint32_t r = current.rows[k];
+      if (r >= i) break;
+      occurrence += current.partner[r] == key ? 1u : 0u;
+    }
+    float force = 0.0f;
+    if (has_memory) {
+      for (std::uint32_t k = memory.offsets[first]; k < memory.offsets[first + 1]; ++k) {
+        const std::uint32_t r = memory.rows[k];
+        if (memory.partner[r] == key) {
+          if (occurrence == 0) {
+            force = memory.multipliers[r];
+            break;
+          }
+          --occurrence;
+        }
+      }
+    }
+    multipliers[i] = force;
+  }
+}
+
+// rotate_axis_angle (cpp/core/mechanics_integration.cpp:9-20).
+__device__ __forceinline__ bool rotate_axis_angle(F3 d, F3 rot, float max_rot, F3& out) {
+  const float mag = norm(rot);
+  if (mag <= 1.0e-12f || max_rot == 0.0f) {
+    out = d;
+    return true;
+  }
+  const float angle = smin(mag, max_rot);
+  const F3 axis = rot * (1.0f / mag);
+  const float c = cosf(angle);
+  const float s = sinf(angle);
+  return normalized(d * c + cross(axis, d) * s + axis * (dot(axis, d) * (1.0f - c)), out);
+}
+
+__global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt,
+                            GeometryBuffers trial, std::uint32_t* rotation_bits, std::uint32_t* invalid,
+                            std::uint32_t* status) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 va = response.a[s];
+    const float4 vb = response.b[s];
+    const F3 rot{vb.x * dt, vb.y * dt, vb.z * dt};
+    if (!finite3(rot)) {
+      atomicExch(invalid, 1u);
+      continue;
+    }
+    const float angle = norm(rot);
+    atomic_max_nonnegative(rotation_bits, angle);
+    if (angle > kMaximumSubstepRotation) {
+      atomicExch(invalid, 1u);
+      continue;
+    }
+    const float4 pl = base.pos_len[s];
+    const float4 dr = base.dir_rad[s];
+    const F3 pos = xyz(pl) + F3{va.x, va.y, va.z} * dt;
+    F3 dir;
+    if (!rotate_axis_angle(xyz(dr), rot, kMaximumSubstepRotation, dir)) {
+      raise_status(status, kStatusGeometry);
+      atomicExch(invalid, 1u);
+      continue;
+    }
+    const float len = pl.w + va.w * dt;
+    if (!finite3(pos) || !finite3(dir) || !isfinite(len) || len < 0.0f) atomicExch(invalid, 1u);
+    trial.pos_len[s] = make_float4(pos.x, pos.y, pos.z, len);
+    trial.dir_rad[s] = make_float4(dir.x, dir.y, dir.z, dr.w);
+  }
+}
+
+__global__ void largest_rotation_kernel(std::uint32_t n, ResponseArrays response, float dt,
+                                        std::uint32_t* rotation_bits) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 vb = response.b[s];
+    const float angle = norm(F3{vb.x * dt, vb.y * dt, vb.z * dt});
+    atomic_max_nonnegative(rotation_bits, isfinite(angle) ? angle : __int_as_float(0x7F800000));
+  }
+}
+
+__global__ void restore_kernel(std::uint32_t n, GeometryBuffers src, GeometryBuffers dst, std::uint32_t* status) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 pl = src.pos_len[s];
+    const float4 dr = src.dir_rad[s];
+    F3 d;
+    if (!finite3(xyz(pl)) || !isfinite(pl.w) || pl.w < 0.0f || !normalized(xyz(dr), d)) {
+      raise_status(status, kStatusGeometry);
+      d = xyz(dr);
+    }
+    dst.pos_len[s] = pl;
+    dst.dir_rad[s] = make_float4(d.x, d.y, d.z, dr.w);
+  }
+}
+
+__global__ void recheck_kernel(const Touch* __restrict__ touches, std::uint32_t count, KeyedLists current,
+                               const float* slack_ptr, float wall_stiffness, float contact_stiffness,
+                               std::uint32_t* __restrict__ flags, std::uint32_t* overlap_bits) {
+  const float slack = *slack_ptr;
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    const Touch t = touches[k];
+    atomic_max_nonnegative(overlap_bits, -t.sep);
+    const bool wall = t.s2 == kInvalidSlot;
+    const std::uint64_t key = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
+    float force = 0.0f;
+    for (std::uint32_t j = current.offsets[t.s1]; j < current.offsets[t.s1 + 1]; ++j) {
+      const std::uint32_t r = current.rows[j];
+      if (current.partner[r] == key) force += current.multipliers[r];
+    }
+    const float compliance = 1.0f / (wall ? wall_stiffness : contact_stiffness);
+    const float allowed = slack + force * compliance;
+    flags[k] = t.sep < -allowed ? 1u : 0u;
+  }
+}
+
+__global__ void gather_flagged_kernel(const Touch* __restrict__ touches, std::uint32_t count,
+                                      const std::uint32_t* __restrict__ flags, const std::uint32_t* __restrict__ offsets,
+                                      Touch* __restrict__ out) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
+    if (flags[k]) out[offsets[k]] = touches[k];
+  }
+}
+
+__global__ void slack_kernel(const std::uint32_t* overlap_bits, float tolerance, float recovery, float* slack) {
+  if (threadIdx.x == 0) {
+    const float starting = __uint_as_float(*overlap_bits);
+    *slack = tolerance + smax(0.0f, starting - recovery);
+  }
+}
+
+__global__ void growth_bound_kernel(std::uint32_t n, GeometryBuffers state, const float* __restrict__ growth, float dt,
+                                    std::uint32_t* bits) {
+  float local = 0.0f;
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float g = fabsf(growth[s]) * state.pos_len[s].w * 0.5f * dt / state.dir_rad[s].w;
+    local = smax(local, g);
+  }
+  for (int o = 16; o > 0; o >>= 1) local = smax(local, __shfl_down_sync(0xFFFFFFFFu, local, o));
+  if ((threadIdx.x & 31) == 0) atomic_max_nonnegative(bits, local);
+}
+
+__global__ void outputs_kernel(std::uint32_t n, ResponseArrays response, GeometryBuffers base, GeometryBuffers initial,
+                               float* velocities, float* loads, float* increments) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    if (velocities != nullptr) {
+      const float4 va = response.a[s];
+      velocities[3 * std::uint64_t(s)] = va.x;
+      velocities[3 * std::uint64_t(s) + 1] = va.y;
+      velocities[3 * std::uint64_t(s) + 2] = va.z;
+    }
+    if (loads != nullptr) loads[s] = response.b[s].w;
+    if (increments != nullptr) increments[s] = base.pos_len[s].w - initial.pos_len[s].w;
+  }
+}
+
+__global__ void copy_loads_kernel(std::uint32_t n, ResponseArrays response, float* loads) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    loads[s] = response.b[s].w;
+  }
+}
+
+__global__ void rows_from_records_kernel(const msb_contact_row* __restrict__ in, std::uint32_t count, RowArrays rows) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const msb_contact_row r = in[i];
+    rows.a[i] = make_float4(r.first_jacobian[0], r.first_jacobian[1], r.first_jacobian[2], r.first_jacobian[3]);
+    rows.b[i] = make_float4(r.first_jacobian[4], r.first_jacobian[5], r.first_length_lever, r.offset);
+    rows.c[i] = make_float4(r.second_jacobian[0], r.second_jacobian[1], r.second_jacobian[2], r.second_jacobian[3]);
+    rows.d[i] = make_float4(r.second_jacobian[4], r.second_jacobian[5], r.second_length_lever, r.compliance);
+    rows.slots[i] = make_uint2(r.first_slot, r.second_slot);
+  }
+}
+
+__global__ void bodies_from_records_kernel(const msb_contact_body* __restrict__ in, std::uint32_t count,
+                                           BodyArrays bodies) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+    const msb_contact_body b = in[i];
+    bodies.a[i] = make_float4(b.axis.x, b.axis.y, b.axis.z, b.translational_mobility);
+    bodies.b[i] = make_float4(b.transverse_mobility, b.axial_mobility, b.length_rate, 0.0f);
+    bodies.drift_a[i] = make_float4(b.drift[0], b.drift[1], b.drift[2], 0.0f);
+    bodies.drift_b[i] = make_float4(b.drift[3], b.drift[4], b.drift[5], 0.0f);
+  }
+}
+
+__global__ void response_layout_kernel(std::uint32_t n, ResponseArrays response, float* velocities, float* loads,
+                                       float* rates) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 va = response.a[s];
+    const float4 vb = response.b[s];
+    if (velocities != nullptr) {
+      float* v = velocities + 6 * std::uint64_t(s);
+      v[0] = va.x;
+      v[1] = va.y;
+      v[2] = va.z;
+      v[3] = vb.x;
+      v[4] = vb.y;
+      v[5] = vb.z;
+    }
+    if (loads != nullptr) loads[s] = vb.w;
+    if (rates != nullptr) rates[s] = va.w;
+  }
+}
+
+}  // namespace
+
+void launch_pack_cells(std::uint32_t n, const float* px, const float* py, const float* pz, const float* dx,
+                       const float* dy, const float* dz, const float* len, const float* radius, GeometryBuffers out,
+                       std::uint32_t* status, cudaStream_t stream) {
+  if (n == 0) return;
+  pack_cells_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, px, py, pz, dx, dy, dz, len, radius, out,
+                                                                     status);
+  count_launch();
+}
+
+void launch_unpack_cells(std::uint32_t n, GeometryBuffers in, float* px, float* py, float* pz, float* dx, float* dy,
+                         float* dz, float* len, cudaStream_t stream) {
+  if (n == 0) return;
+  unpack_cells_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, in, px, py, pz, dx, dy, dz, len);
+  count_launch();
+}
+
+void launch_make_bodies(std::uint32_t n, GeometryBuffers state, const float* growth_rates, const std::uint8_t* fixed,
+                        GeometryBuffers rate_lengths, float drag, BodyArrays bodies, cudaStream_t stream) {
+  if (n == 0) return;
+  make_bodies_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, state, growth_rates, fixed, rate_lengths,
+                                                                      drag, bodies);
+  count_launch();
+}
+
+void launch_make_rows(const Touch* touches, std::uint32_t count, GeometryBuffers geometry, RowBuild prm,
+                      const ResponseArrays* response, RowArrays rows, std::uint32_t row_base,
+                      std::uint64_t* key_partner, float* multipliers, std::uint32_t* overlap_bits,
+                      cudaStream_t stream) {
+  if (count == 0) return;
+  const ResponseArrays none{nullptr, nullptr};
+  make_rows_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(
+      touches, count, geometry, prm, response != nullptr ? *response : none, response != nullptr ? 1 : 0, rows,
+      row_base, key_partner, multipliers, overlap_bits);
+  count_launch();
+}
+
+void launch_warm_start(std::uint32_t rows, const uint2* slots, KeyedLists current, const KeyedLists* memory,
+                       float* multipliers, cudaStream_t stream) {
+  if (rows == 0) return;
+  const KeyedLists none{nullptr, nullptr, nullptr, nullptr};
+  warm_start_kernel<<<grid_for(rows, kThreads), kThreads, 0, stream>>>(
+      rows, slots, current, memory != nullptr ? *memory : none, memory != nullptr ? 1 : 0, multipliers);
+  count_launch();
+}
+
+void launch_move(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt, GeometryBuffers trial,
+                 std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream) {
+  if (n == 0) return;
+  move_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, base, response, dt, trial, rotation_bits, invalid,
+                                                               status);
+  count_launch();
+}
+
+void launch_largest_rotation(std::uint32_t n, ResponseArrays response, float dt, std::uint32_t* rotation_bits,
+                             cudaStream_t stream) {
+  if (n == 0) return;
+  largest_rotation_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, response, dt, rotation_bits);
+  count_launch();
+}
+
+void launch_restore(std::uint32_t n, GeometryBuffers src, GeometryBuffers dst, std::uint32_t* status,
+                    cudaStream_t stream) {
+  if (n == 0) return;
+  restore_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, src, dst, status);
+  count_launch();
+}
+
+void launch_recheck(const Touch* touches, std::uint32_t count, KeyedLists current, const float* slack,
+                    float wall_stiffness, float contact_stiffness, std::uint32_t* flags, std::uint32_t* overlap_bits,
+                    cudaStream_t stream) {
+  if (count == 0) return;
+  recheck_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(touches, count, current, slack, wall_stiffness,
+                                                                      contact_stiffness, flags, overlap_bits);
+  count_launch();
+}
+
+void launch_gather_flagged(const Touch* touches, std::uint32_t count, const std::uint32_t* flags,
+                           const std::uint32_t* offsets, Touch* out, cudaStream_t stream) {
+  if (count == 0) return;
+  gather_flagged_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(touches, count, flags, offsets, out);
+  count_launch();
+}
+
+void launch_slack(const std::uint32_t* overlap_bits, float tolerance, float recovery, float* slack,
+                  cudaStream_t stream) {
+  slack_kernel<<<1, 32, 0, stream>>>(overlap_bits, tolerance, recovery, slack);
+  count_launch();
+}
+
+void launch_growth_bound(std::uint32_t n, GeometryBuffers state, const float* growth_rates, float dt,
+                         std::uint32_t* bits, cudaStream_t stream) {
+  if (n == 0) return;
+  growth_bound_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, state, growth_rates, dt, bits);
+  count_launch();
+}
+
+void launch_outputs(std::uint32_t n, ResponseArrays response, GeometryBuffers base, GeometryBuffers initial,
+                    float* velocities, float* loads, float* increments, cudaStream_t stream) {
+  if (n == 0) return;
+  outputs_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, response, base, initial, velocities, loads,
+                                                                  increments);
+  count_launch();
+}
+
+void launch_copy_loads(std::uint32_t n, ResponseArrays response, float* loads, cudaStream_t stream) {
+  if (n == 0) return;
+  copy_loads_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, response, loads);
+  count_launch();
+}
+
+void launch_rows_from_records(const void* records, std::uint32_t count, RowArrays rows, cudaStream_t stream) {
+  if (count == 0) return;
+  rows_from_records_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(
+      static_cast<const msb_contact_row*>(records), count, rows);
+  count_launch();
+}
+
+void launch_bodies_from_records(const void* records, std::uint32_t count, BodyArrays bodies, cudaStream_t stream) {
+  if (count == 0) return;
+  bodies_from_records_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(
+      static_cast<const msb_contact_body*>(records), count, bodies);
+  count_launch();
+}
+
+void launch_response_to_host_layout(std::uint32_t n, ResponseArrays response, float* velocities, float* loads,
+                                    float* rates, cudaStream_t stream) {
+  if (n == 0) return;
+  response_layout_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, response, velocities, loads, rates);
+  count_launch();
+}
+
+}  // namespace msb

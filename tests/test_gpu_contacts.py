@@ -1,0 +1,125 @@
+"""Contact detection on the GPU through the C-ABI, against the reference's
+golden fixtures and the FP32 oracle: pair lists, separations, points,
+normals and weights bit-exact."""
+
+import numpy as np
+import pytest
+
+from microsimulator_b200 import abi, workloads
+from microsimulator_b200.simulation import contact_incidence
+from microsimulator_b200.types import ConstraintContactParameters, ContactParameters
+from microsimulator_b200.world import WorldState
+from tests.golden.make_golden import wall_set, world_from
+
+pytestmark = pytest.mark.gpu
+
+
+def test_geometry_kats_bit_exact(backend, golden):
+    data = golden("geometry_kat")
+    for name in data["names"]:
+        world = world_from(data, f"{name}__")
+        for margin in (0.01, 0.1):
+            expected = data[f"{name}__contacts_{margin}"]
+            actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=margin))
+            assert actual.tobytes() == expected.tobytes(), (name, margin)
+
+
+def test_empty_and_single_cell(backend):
+    assert len(backend.find_cell_contacts(WorldState())) == 0
+    w = WorldState()
+    w.add_cell((0, 0, 0), (1, 0, 0), 2.0, 0.5)
+    assert len(backend.find_cell_contacts(w)) == 0
+
+
+def test_grid_matches_exhaustive_257(backend, golden):
+    data = golden("pseudo_random_257")
+    world = world_from(data, "world__")
+    for margin in (0.0, 0.01, 0.5):
+        actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=margin))
+        assert actual.tobytes() == data[f"contacts_{margin}"].tobytes()
+
+
+def test_colony_contacts_and_incidence(backend, golden):
+    data = golden("colony_1k")
+    world = world_from(data, "world__")
+    actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=0.1))
+    assert actual.tobytes() == data["contacts_0.1"].tobytes()
+    offsets, indices = contact_incidence(actual, len(world))
+    assert np.array_equal(offsets, data["incidence_offsets"].astype(np.int64))
+    assert np.array_equal(indices, data["incidence_indices"].astype(np.int64))
+
+
+def test_walls_bit_exact(backend, golden):
+    data = golden("walls")
+    world = world_from(golden("colony_1k"), "world__")
+    cs = wall_set()
+    for every_face in (0, 1):
+        for margin in (0.0, 0.1):
+            actual = backend.find_external_contacts(world, cs, ConstraintContactParameters(margin),
+                                                    every_face=bool(every_face))
+            assert actual.tobytes() == data[f"walls_{every_face}_{margin}"].tobytes(), (every_face, margin)
+
+
+def test_dense_pile_many_partners(backend, oracle):
+    # More than 32 partners per cell takes the global-memory sort.
+    w = WorldState()
+    rng = np.random.default_rng(1)
+    for k in range(80):
+        w.add_cell(tuple(rng.uniform(-0.3, 0.3, 3)), tuple(rng.normal(size=3)), 2.0, 0.5)
+    expected = oracle.find_cell_contacts(w, ContactParameters(activation_margin=0.1))
+    actual = backend.find_cell_contacts(w, ContactParameters(activation_margin=0.1))
+    assert actual.tobytes() == expected.tobytes()
+
+
+def test_sparse_cells_use_hashed_grid(backend, oracle):
+    # Cells spread so thinly that a dense grid would exceed 8N + 4096 boxes.
+    w = WorldState()
+    rng = np.random.default_rng(2)
+    pos = rng.uniform(-5000, 5000, (3000, 3))
+    pos[:10] = [(0.1 * k, 0, 0) for k in range(10)]
+    w = WorldState.from_arrays(pos, rng.normal(size=(3000, 3)), 2.0, 0.5)
+    expected = oracle.find_cell_contacts(w, ContactParameters(activation_margin=0.1))
+    actual = backend.find_cell_contacts(w, ContactParameters(activation_margin=0.1))
+    assert len(expected) > 0
+    assert actual.tobytes() == expected.tobytes()
+
+
+def test_ids_out_of_slot_order_and_wide_ids(backend, oracle):
+    world = workloads.colony_1k(seed=11, n=2000, side=60.0)
+    rng = np.random.default_rng(3)
+    world.ids = (rng.permutation(len(world)).astype(np.uint64) + np.uint64(1)) * np.uint64(3_000_000_007)
+    expected = oracle.find_cell_contacts(world, ContactParameters(activation_margin=0.1))
+    actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=0.1))
+    assert actual.tobytes() == expected.tobytes()
+
+
+@pytest.mark.parametrize("n", [20_000, 200_000])
+def test_jammed_colony_contacts_bit_exact(backend, oracle, n):
+    world = workloads.jammed(n=n, seed=5)
+    for margin in (0.0, 0.1):
+        expected = oracle.find_cell_contacts(world, ContactParameters(activation_margin=margin))
+        actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=margin))
+        assert actual.tobytes() == expected.tobytes()
+
+
+def test_trap_walls_bit_exact(backend, oracle):
+    world, cs = workloads.trap_colony(n=5000, seed=4)
+    for every_face in (False, True):
+        expected = oracle.find_external_contacts(world, cs, ConstraintContactParameters(0.1), every_face=every_face)
+        actual = backend.find_external_contacts(world, cs, ConstraintContactParameters(0.1), every_face=every_face)
+        assert actual.tobytes() == expected.tobytes()
+
+
+def test_invalid_inputs_raise(backend):
+    w = WorldState()
+    w.add_cell((0, 0, 0), (1, 0, 0), 2.0, 0.5)
+    w.add_cell((1, 0, 0), (1, 0, 0), 2.0, 0.5)
+    with pytest.raises(ValueError):
+        backend.find_cell_contacts(w, ContactParameters(parallel_sine_threshold=2.0))
+    w.ids[1] = w.ids[0]
+    with pytest.raises(ValueError):
+        backend.find_cell_contacts(w)
+    w.ids[1] = 2
+    w.position_x[0] = np.nan
+    with pytest.raises(ValueError):
+        backend.find_cell_contacts(w)
