@@ -235,7 +235,7 @@ class DeviceCells:
         import torch
 
         def up(array, dtype):
-            return torch.from_numpy(np.ascontiguousarray(array)).to(device=device, dtype=dtype)
+            return torch.from_numpy(np.array(array)).to(device=device, dtype=dtype)
 
         self.count = len(world)
         self.ids = up(world.ids.view(np.int64), torch.int64)

@@ -81,16 +81,16 @@ class WorldState:
         directions = np.asarray(directions, dtype=f32).reshape(-1, 3)
         n = positions.shape[0]
         dx, dy, dz = normalized_arrays(directions[:, 0], directions[:, 1], directions[:, 2])
-        world.position_x = np.ascontiguousarray(positions[:, 0])
-        world.position_y = np.ascontiguousarray(positions[:, 1])
-        world.position_z = np.ascontiguousarray(positions[:, 2])
+        world.position_x = np.array(positions[:, 0])
+        world.position_y = np.array(positions[:, 1])
+        world.position_z = np.array(positions[:, 2])
         world.direction_x, world.direction_y, world.direction_z = dx.copy(), dy.copy(), dz.copy()
-        world.lengths = np.ascontiguousarray(np.broadcast_to(np.asarray(lengths, dtype=f32), (n,)))
-        world.radii = np.ascontiguousarray(np.broadcast_to(np.asarray(radii, dtype=f32), (n,)))
+        world.lengths = np.array(np.broadcast_to(np.asarray(lengths, dtype=f32), (n,)))
+        world.radii = np.array(np.broadcast_to(np.asarray(radii, dtype=f32), (n,)))
         rates = 1.0 if growth_rates is None else growth_rates
-        world.growth_rates = np.ascontiguousarray(np.broadcast_to(np.asarray(rates, dtype=f32), (n,)))
+        world.growth_rates = np.array(np.broadcast_to(np.asarray(rates, dtype=f32), (n,)))
         fixed = 0 if fixed is None else fixed
-        world.fixed = np.ascontiguousarray(np.broadcast_to(np.asarray(fixed, dtype=np.uint8), (n,)))
+        world.fixed = np.array(np.broadcast_to(np.asarray(fixed, dtype=np.uint8), (n,)))
         if ids is None:
             world.ids = np.arange(1, n + 1, dtype=np.uint64)
         else:
@@ -170,7 +170,11 @@ class WorldState:
         fraction = f32(first_fraction)
         if not (0 < fraction < 1):
             raise ValueError("first daughter fraction must be between zero and one")
-        slots = np.array([self.slot_of(int(i)) for i in parent_ids], dtype=np.int64)
+        order = np.argsort(self.ids, kind="stable")
+        where = np.searchsorted(self.ids[order], parent_ids)
+        if np.any(where >= len(self)) or np.any(self.ids[order[np.minimum(where, len(self) - 1)]] != parent_ids):
+            raise KeyError("unknown parent id")
+        slots = order[where].astype(np.int64)
         length = self.lengths[slots]
         radius = self.radii[slots]
         available = (length - (f32(2.0) * radius)).astype(f32)
