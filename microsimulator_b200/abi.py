@@ -372,6 +372,17 @@ SIGNATURES = {
         ],
     ),
     "msb_launch_count": (c_uint64, [c_void_p]),
+    "msb_solve_contact_forces_no_alloc": (
+        c_int,
+        [
+            POINTER(ContactSystem),
+            c_void_p,
+            POINTER(ContactSolveParameters),
+            c_void_p,
+            POINTER(ContactSolveReport),
+            c_void_p,
+        ],
+    ),
     "msb_profile_iterations": (
         c_int,
         [c_void_p, c_uint32, POINTER(c_float), POINTER(c_float), POINTER(c_uint64), POINTER(c_uint64)],
