@@ -75,46 +75,76 @@ def divide(world, step, seed):
 
 
 class Clocks:
-    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    """SM clock and throttle reasons sampled through NVML from a background
+    thread during a region (every 0.5 s, one device).  An external
+    `nvidia-smi -lms` poller takes driver locks often enough to stall the
+    step's host synchronizations, so the sampling stays in-process and light."""
 
-    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
 
-    def __init__(self, device):
+    def __init__(self, device, period=0.5):
         self.device = device
-        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
-        self.proc = None
+        self.period = period
+        self.samples = []
+        self._stop = None
+        self._thread = None
+        self._handle = None
+        self._max = None
 
     def __enter__(self):
+        import threading
+
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
-        except FileNotFoundError:
-            self.proc = None
+            import pynvml
+            import torch
+
+            pynvml.nvmlInit()
+            props = torch.cuda.get_device_properties(self.device)
+            want = (int(props.pci_domain_id), int(props.pci_bus_id), int(props.pci_device_id))
+            # Match on NVML's PCI info (integers): the bus-id lookup takes a
+            # string, and CUDA_VISIBLE_DEVICES may renumber the devices.
+            for index in range(pynvml.nvmlDeviceGetCount()):
+                handle = pynvml.nvmlDeviceGetHandleByIndex(index)
+                pci = pynvml.nvmlDeviceGetPciInfo(handle)
+                if (int(pci.domain), int(pci.bus), int(pci.device)) == want:
+                    self._handle = handle
+                    break
+            if self._handle is None:
+                return self
+            self._max = pynvml.nvmlDeviceGetMaxClockInfo(self._handle, pynvml.NVML_CLOCK_SM)
+        except Exception:
+            self._handle = None
+            return self
+        self._stop = threading.Event()
+
+        def run():
+            import pynvml
+
+            while True:
+                try:
+                    sm = pynvml.nvmlDeviceGetClockInfo(self._handle, pynvml.NVML_CLOCK_SM)
+                    reasons = pynvml.nvmlDeviceGetCurrentClocksEventReasons(self._handle)
+                    self.samples.append((sm, reasons))
+                except Exception:
+                    pass
+                if self._stop.wait(self.period):
+                    break
+
+        self._thread = threading.Thread(target=run, daemon=True)
+        self._thread.start()
         return self
 
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
-            try:
-                self.proc.wait(timeout=5)
-            except subprocess.TimeoutExpired:
-                self.proc.kill()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
 
     def summary(self):
-        self.file.flush()
-        rows = [line.split(",") for line in Path(self.file.name).read_text().splitlines() if line.strip()]
-        if not rows:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
-        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if len(r) > 5 + k and "Active" in r[5 + k]
-                          and "Not" not in r[5 + k]})
-        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
-                "reasons": reasons, "samples": len(rows)}
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self._max, "reasons": ["unsampled"], "samples": 0}
+        reasons = sorted({name for _, bits in self.samples for mask, name in self.REASONS.items() if bits & mask})
+        return {"sm_mhz": float(np.median([s for s, _ in self.samples])), "sm_max_mhz": self._max,
+                "reasons": reasons, "samples": len(self.samples), "source": "nvml"}
 
 
 def measured_peak():
@@ -256,13 +286,15 @@ def main():
     total_ms = 0.0
     cell_steps = 0
     iterations = 0
+    phases = {name: 0.0 for name in backend.PHASES}
     with Clocks(local) as clocks:
         for k in range(args.steps):
-            n_before = len(world)
             ms, report = device_step(args.warmup + k)
             total_ms += ms
-            cell_steps += len(world)
+            cell_steps += len(world)  # the cells of the step (divisions run before it)
             iterations += report.iterations
+            for name, value in backend.last_step_phases().items():
+                phases[name] += value / args.steps
     barrier()
     launches = backend.launch_count() - launches0
     prof = backend.profile_iterations(20)
@@ -332,6 +364,7 @@ def main():
             "config": config(args, world_size),
             "path": "plain",
             "bb_iterations_per_step": iterations / args.steps,
+            "phase_ms_per_step": phases,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",
                 "bound": "hbm",

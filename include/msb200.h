@@ -362,6 +362,15 @@ int msb_advance_contact_dynamics_device(
 int msb_profile_iterations(msb_context* context, uint32_t iterations, float* body_ms, float* row_ms,
                            uint64_t* rows, uint64_t* bodies);
 
+/* Device time of the last msb_advance_contact_dynamics(_device) call by
+ * phase, measured with CUDA events on the context's stream, in
+ * milliseconds: [0] upload, validation and id order; [1] contact searches;
+ * [2] bodies, rows, keys and warm start; [3] incidence builds; [4] BB solves;
+ * [5] moves and overlap re-checks; [6] outputs and download.  Writes
+ * min(capacity, 7) values.  A measurement aid with no counterpart in the
+ * reference. */
+int msb_last_step_phases(const msb_context* context, double* milliseconds, uint32_t capacity);
+
 /* Kernel launches issued by this context since it was created (for the
  * launch counts that benchmarks report). */
 uint64_t msb_launch_count(const msb_context* context);

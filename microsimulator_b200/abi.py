@@ -372,6 +372,7 @@ SIGNATURES = {
         ],
     ),
     "msb_launch_count": (c_uint64, [c_void_p]),
+    "msb_last_step_phases": (c_int, [c_void_p, c_void_p, c_uint32]),
     "msb_solve_contact_forces_no_alloc": (
         c_int,
         [

@@ -79,6 +79,14 @@ class B200Backend:
     def launch_count(self) -> int:
         return int(self._lib.msb_launch_count(self._handle))
 
+    PHASES = ("load", "search", "rows", "incidence", "solve", "move", "output")
+
+    def last_step_phases(self) -> dict:
+        """Device milliseconds of the last step by phase (CUDA events)."""
+        out = np.zeros(len(self.PHASES), dtype=np.float64)
+        self._check(self._lib.msb_last_step_phases(self._handle, c_void_p(abi.ptr(out)), len(out)))
+        return dict(zip(self.PHASES, out.tolist()))
+
     def profile_iterations(self, iterations: int = 20) -> dict:
         """Mean device time of one BB iteration's body and row passes on the
         last solved system (CUDA events on the backend's stream)."""

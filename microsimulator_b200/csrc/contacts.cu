@@ -78,14 +78,31 @@ __global__ void cell_bounds_kernel(GeometryView g, float margin, double* __restr
 
 __global__ void grid_setup_kernel(const double* __restrict__ partials, std::uint32_t partial_count,
                                   std::uint32_t cells, std::uint64_t bucket_capacity, GridParams* grid) {
-  if (threadIdx.x != 0) return;
+  // Block reduction of the per-block partials (minima, maxima, finite flag).
+  __shared__ double shared[10][kThreads / 32];
   double v[10];
-  for (int k = 0; k < 10; ++k) v[k] = partials[k];
-  for (std::uint32_t p = 1; p < partial_count; ++p) {
+  for (int k = 0; k < 10; ++k) v[k] = (k < 3 || k == 9) ? DBL_MAX : -DBL_MAX;
+  v[6] = v[7] = v[8] = 0.0;
+  for (std::uint32_t p = threadIdx.x; p < partial_count; p += blockDim.x) {
     for (int k = 0; k < 10; ++k) {
       const double x = partials[10 * p + k];
       v[k] = (k < 3 || k == 9) ? fmin(v[k], x) : fmax(v[k], x);
     }
+  }
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  for (int k = 0; k < 10; ++k) {
+    for (int o = 16; o > 0; o >>= 1) {
+      const double other = __shfl_down_sync(0xFFFFFFFFu, v[k], o);
+      v[k] = (k < 3 || k == 9) ? fmin(v[k], other) : fmax(v[k], other);
+    }
+    if (lane == 0) shared[k][warp] = v[k];
+  }
+  __syncthreads();
+  if (threadIdx.x != 0) return;
+  for (int k = 0; k < 10; ++k) {
+    v[k] = shared[k][0];
+    for (int w = 1; w < kThreads / 32; ++w) v[k] = (k < 3 || k == 9) ? fmin(v[k], shared[k][w]) : fmax(v[k], shared[k][w]);
   }
   GridParams out{};
   out.status = v[9] > 0.5 ? 0u : 1u;
@@ -166,12 +183,22 @@ __global__ void bin_cells_kernel(GeometryView g, const double* __restrict__ boun
   }
 }
 
-__global__ void scatter_cells_kernel(std::uint32_t cells, const std::uint32_t* __restrict__ cell_bucket,
+// Places each cell at its bucket's next position, with its box rounded
+// outward to FP32 (a box that overlaps in FP64 overlaps in these), its slot
+// in lo.w and its id: the sweep then reads a bucket's cells contiguously.
+__global__ void scatter_cells_kernel(GeometryView g, const double* __restrict__ bounds,
+                                     const std::uint32_t* __restrict__ cell_bucket,
                                      const std::uint32_t* __restrict__ starts, std::uint32_t* __restrict__ fill,
-                                     std::uint32_t* __restrict__ members) {
-  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cells; i += gridDim.x * blockDim.x) {
+                                     float4* __restrict__ sorted_lo, float4* __restrict__ sorted_hi,
+                                     std::uint64_t* __restrict__ sorted_id) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.count; i += gridDim.x * blockDim.x) {
     const std::uint32_t b = cell_bucket[i];
-    members[starts[b] + atomicAdd(&fill[b], 1u)] = i;
+    const std::uint32_t at = starts[b] + atomicAdd(&fill[b], 1u);
+    const double* box = bounds + 6 * std::uint64_t(i);
+    sorted_lo[at] = make_float4(__double2float_rd(box[0]), __double2float_rd(box[1]), __double2float_rd(box[2]),
+                                __uint_as_float(i));
+    sorted_hi[at] = make_float4(__double2float_ru(box[3]), __double2float_ru(box[4]), __double2float_ru(box[5]), 0.0f);
+    sorted_id[at] = g.ids[i];
   }
 }
 
@@ -181,28 +208,35 @@ __device__ __forceinline__ bool boxes_overlap(const double* l, const double* r) 
 
 constexpr int kLocalPartners = 32;
 
-// One thread per cell: its partners of higher id among the cells of the 27
-// (or fewer) grid boxes around it whose padded boxes overlap its own.
+// One thread per cell, cells taken in bucket order so that a warp's cells
+// share their neighbour buckets in cache: the partners of higher id among
+// the cells of the 27 (or fewer) grid boxes around it whose padded boxes
+// overlap its own.  The FP32 outward-rounded boxes cull; the reference's
+// FP64 box test decides (cpp/core/contact_graph.cpp:37-41).
 __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bounds, const GridParams* grid_ptr,
-                                   const std::uint32_t* __restrict__ starts, const std::uint32_t* __restrict__ members,
+                                   const std::uint32_t* __restrict__ starts, const float4* __restrict__ sorted_lo,
+                                   const float4* __restrict__ sorted_hi, const std::uint64_t* __restrict__ sorted_id,
                                    const std::int64_t* __restrict__ coords, const std::uint32_t* __restrict__ rank,
                                    std::uint32_t* __restrict__ counts, const std::uint32_t* __restrict__ offsets,
                                    uint2* __restrict__ pairs, std::uint32_t* status) {
   const GridParams grid = *grid_ptr;
   if (grid.status != 0) return;
   const bool fill = pairs != nullptr;
-  for (std::uint32_t a = blockIdx.x * blockDim.x + threadIdx.x; a < g.count; a += gridDim.x * blockDim.x) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < g.count; k += gridDim.x * blockDim.x) {
+    const float4 my_lo = sorted_lo[k];
+    const float4 my_hi = sorted_hi[k];
+    const std::uint32_t a = __float_as_uint(my_lo.w);
+    const std::uint64_t id = sorted_id[k];
     double box[6];
 #pragma unroll
-    for (int k = 0; k < 6; ++k) box[k] = bounds[6 * std::uint64_t(a) + k];
-    const std::uint64_t id = g.ids[a];
+    for (int q = 0; q < 6; ++q) box[q] = bounds[6 * std::uint64_t(a) + q];
     std::int64_t at[3];
     box_of(box, grid, at);
     std::int64_t first[3], last[3];
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      first[k] = at[k] == 0 ? 0 : at[k] - 1;
-      last[k] = smin(std::int64_t(grid.dims[k]) - 1, at[k] + 1);
+    for (int q = 0; q < 3; ++q) {
+      first[q] = at[q] == 0 ? 0 : at[q] - 1;
+      last[q] = smin(std::int64_t(grid.dims[q]) - 1, at[q] + 1);
     }
     const std::uint32_t base = fill ? offsets[rank[a]] : 0;
     std::uint32_t found = 0;
@@ -214,13 +248,19 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
           const std::uint32_t b = bucket_of(grid, x, y, z);
           const std::uint32_t end = starts[b + 1];
           for (std::uint32_t m = starts[b]; m < end; ++m) {
-            const std::uint32_t j = members[m];
+            const std::uint64_t other = sorted_id[m];
+            if (!(other > id)) continue;
+            const float4 lo = sorted_lo[m];
+            const float4 hi = sorted_hi[m];
+            if (!(my_hi.x >= lo.x && hi.x >= my_lo.x && my_hi.y >= lo.y && hi.y >= my_lo.y && my_hi.z >= lo.z &&
+                  hi.z >= my_lo.z)) {
+              continue;
+            }
+            const std::uint32_t j = __float_as_uint(lo.w);
             if (grid.hashed) {
               const std::int64_t* c = coords + 3 * std::uint64_t(j);
               if (c[0] != x || c[1] != y || c[2] != z) continue;
             }
-            const std::uint64_t other = g.ids[j];
-            if (!(other > id)) continue;
             if (!boxes_overlap(box, bounds + 6 * std::uint64_t(j))) continue;
             if (fill) {
               if (found < kLocalPartners) {
@@ -851,7 +891,7 @@ void launch_cell_bounds(GeometryView g, float margin, double* bounds, double* pa
 
 void launch_grid_setup(const double* partials, std::uint32_t partial_count, std::uint32_t cells,
                        std::uint64_t bucket_capacity, GridParams* grid, cudaStream_t stream) {
-  grid_setup_kernel<<<1, 32, 0, stream>>>(partials, partial_count, cells, bucket_capacity, grid);
+  grid_setup_kernel<<<1, kThreads, 0, stream>>>(partials, partial_count, cells, bucket_capacity, grid);
   count_launch();
 }
 
@@ -862,20 +902,23 @@ void launch_bin_cells(GeometryView g, const double* bounds, const GridParams* gr
   count_launch();
 }
 
-void launch_scatter_cells(std::uint32_t cells, const std::uint32_t* cell_bucket, const std::uint32_t* bucket_starts,
-                          std::uint32_t* bucket_fill, std::uint32_t* members, cudaStream_t stream) {
-  scatter_cells_kernel<<<grid_for(cells, kThreads), kThreads, 0, stream>>>(cells, cell_bucket, bucket_starts,
-                                                                            bucket_fill, members);
+void launch_scatter_cells(GeometryView g, const double* bounds, const std::uint32_t* cell_bucket,
+                          const std::uint32_t* bucket_starts, std::uint32_t* bucket_fill, float4* sorted_lo,
+                          float4* sorted_hi, std::uint64_t* sorted_id, cudaStream_t stream) {
+  scatter_cells_kernel<<<grid_for(g.count, kThreads), kThreads, 0, stream>>>(g, bounds, cell_bucket, bucket_starts,
+                                                                              bucket_fill, sorted_lo, sorted_hi,
+                                                                              sorted_id);
   count_launch();
 }
 
 void launch_broad_phase(GeometryView g, const double* bounds, const GridParams* grid,
-                        const std::uint32_t* bucket_starts, const std::uint32_t* members,
-                        const std::int64_t* cell_coords, const std::uint32_t* rank, std::uint32_t* counts,
-                        const std::uint32_t* offsets, uint2* pairs, std::uint32_t* status, cudaStream_t stream) {
-  broad_phase_kernel<<<grid_for(g.count, 128, 16), 128, 0, stream>>>(g, bounds, grid, bucket_starts, members,
-                                                                      cell_coords, rank, counts, offsets, pairs,
-                                                                      status);
+                        const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
+                        const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* rank,
+                        std::uint32_t* counts, const std::uint32_t* offsets, uint2* pairs, std::uint32_t* status,
+                        cudaStream_t stream) {
+  broad_phase_kernel<<<grid_for(g.count, 128, 16), 128, 0, stream>>>(g, bounds, grid, bucket_starts, sorted_lo,
+                                                                      sorted_hi, sorted_id, cell_coords, rank, counts,
+                                                                      offsets, pairs, status);
   count_launch();
 }
 

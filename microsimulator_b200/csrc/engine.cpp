@@ -74,11 +74,14 @@ struct DBuf {
     p = nullptr;
     cap = 0;
   }
+  // Capacity for n elements: a quarter of headroom, rounded up to a power of
+  // two, so that a colony growing by divisions does not reallocate each step.
+  static std::size_t capacity_for(std::size_t n) { return std::bit_ceil(std::max<std::size_t>(n + n / 4, 64)); }
   // Grows to at least n elements; contents are not kept.
   T* ensure(std::size_t n) {
     if (n > cap) {
       release();
-      const std::size_t c = std::bit_ceil(std::max<std::size_t>(n, 64));
+      const std::size_t c = capacity_for(n);
       check(cudaMalloc(&p, c * sizeof(T)), "cudaMalloc");
       cap = c;
     }
@@ -87,7 +90,7 @@ struct DBuf {
   // Grows to at least n elements keeping the first `keep`.
   T* grow(std::size_t n, std::size_t keep, cudaStream_t stream) {
     if (n <= cap) return p;
-    const std::size_t c = std::bit_ceil(std::max<std::size_t>(n, 64));
+    const std::size_t c = capacity_for(n);
     T* q = nullptr;
     check(cudaMalloc(&q, c * sizeof(T)), "cudaMalloc");
     if (keep > 0) check(cudaMemcpyAsync(q, p, keep * sizeof(T), cudaMemcpyDeviceToDevice, stream), "grow copy");
@@ -305,7 +308,9 @@ struct msb_context {
   // contact search
   msb::DBuf<double> bounds, bound_partials;
   msb::DBuf<msb::GridParams> grid;
-  msb::DBuf<std::uint32_t> cell_bucket, bucket_counts, bucket_starts, bucket_fill, members;
+  msb::DBuf<std::uint32_t> cell_bucket, bucket_counts, bucket_starts, bucket_fill;
+  msb::DBuf<float4> sorted_lo, sorted_hi;
+  msb::DBuf<std::uint64_t> sorted_id;
   msb::DBuf<std::int64_t> coords;
   msb::DBuf<std::uint32_t> cand_counts, cand_offsets, pair_counts, pair_offsets, wall_counts, wall_offsets;
   msb::DBuf<uint2> pairs;
@@ -317,6 +322,7 @@ struct msb_context {
   // the contact system
   msb::RowStore rows, memory;
   bool has_memory = false;
+  bool has_drift = false;  // a loaded system with some non-zero drift
   msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
   msb::DBuf<std::uint32_t> inc_offsets;
   msb::DBuf<float4> inc_a, inc_b, resp_a, resp_b, accepted_a, accepted_b;
@@ -333,6 +339,11 @@ struct msb_context {
   std::uint32_t* host_scalars = nullptr;
   msb::SolveDesc* host_desc = nullptr;
 
+  // phase timing of the last step: events at phase boundaries
+  std::vector<cudaEvent_t> phase_events;
+  std::vector<int> phase_marks;
+  std::array<double, 8> phase_ms{};
+
   // outputs staging for host calls
   msb::DBuf<float> out_velocities, out_loads, out_increments;
   msb::DBuf<std::uint8_t> records;
@@ -342,6 +353,41 @@ namespace msb {
 namespace {
 
 using Ctx = msb_context;
+
+// Phases of a step, in the order msb_last_step_phases reports them.
+enum Phase : int {
+  kPhaseLoad = 0,       // upload, validation, id order
+  kPhaseSearch = 1,     // cell list, broad and narrow phase, wall contacts
+  kPhaseRows = 2,       // bodies, rows, keys, warm start, refinement rows
+  kPhaseIncidence = 3,  // per-body incidence of the rows
+  kPhaseSolve = 4,      // the BB solves
+  kPhaseMove = 5,       // move, restore, overlap re-check
+  kPhaseOutput = 6,     // outputs and download
+  kPhaseEnd = 7
+};
+
+// Records an event on the stream where `phase` begins (the previous phase ends).
+void mark(Ctx& c, int phase) {
+  if (c.phase_marks.size() == c.phase_events.size()) {
+    cudaEvent_t e;
+    check(cudaEventCreate(&e), "event");
+    c.phase_events.push_back(e);
+  }
+  check(cudaEventRecord(c.phase_events[c.phase_marks.size()], c.stream), "event");
+  c.phase_marks.push_back(phase);
+}
+
+void collect_phases(Ctx& c) {
+  c.phase_ms.fill(0.0);
+  if (c.phase_marks.empty()) return;
+  check(cudaEventSynchronize(c.phase_events[c.phase_marks.size() - 1]), "event");
+  for (std::size_t k = 0; k + 1 < c.phase_marks.size(); ++k) {
+    float ms = 0.0f;
+    check(cudaEventElapsedTime(&ms, c.phase_events[k], c.phase_events[k + 1]), "event");
+    c.phase_ms[c.phase_marks[k]] += ms;
+  }
+  c.phase_marks.clear();
+}
 
 void sync(Ctx& c) { check(cudaStreamSynchronize(c.stream), "stream"); }
 
@@ -487,19 +533,22 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   c.bucket_counts.ensure(capacity);
   c.bucket_starts.ensure(capacity);
   c.bucket_fill.ensure(capacity);
-  c.members.ensure(n);
+  c.sorted_lo.ensure(n);
+  c.sorted_hi.ensure(n);
+  c.sorted_id.ensure(n);
   c.temp.ensure(scan_temp_words(capacity) + sort_temp_words(n) + 64);
   check(cudaMemsetAsync(c.bucket_counts.p, 0, capacity * 4, c.stream), "memset");
   check(cudaMemsetAsync(c.bucket_fill.p, 0, capacity * 4, c.stream), "memset");
   launch_bin_cells(g, c.bounds.p, c.grid.p, c.cell_bucket.p, c.coords.p, c.bucket_counts.p, c.stream);
   exclusive_scan(c.bucket_counts.p, c.bucket_starts.p, capacity, c.temp.p, c.stream);
-  launch_scatter_cells(n, c.cell_bucket.p, c.bucket_starts.p, c.bucket_fill.p, c.members.p, c.stream);
+  launch_scatter_cells(g, c.bounds.p, c.cell_bucket.p, c.bucket_starts.p, c.bucket_fill.p, c.sorted_lo.p, c.sorted_hi.p,
+                       c.sorted_id.p, c.stream);
   c.cand_counts.ensure(n + 1ull);
   c.cand_offsets.ensure(n + 1ull);
   check(cudaMemsetAsync(c.cand_counts.p + n, 0, 4, c.stream), "memset");
   reset_scalars(c);
-  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.members.p, c.coords.p, c.rank.p, c.cand_counts.p,
-                     nullptr, nullptr, c.scalars.p + kStatus, c.stream);
+  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
+                     c.coords.p, c.rank.p, c.cand_counts.p, nullptr, nullptr, c.scalars.p + kStatus, c.stream);
   exclusive_scan(c.cand_counts.p, c.cand_offsets.p, n + 1ull, c.temp.p, c.stream);
   // grid status and the candidate total
   GridParams grid{};
@@ -512,8 +561,9 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   const std::uint32_t pair_count = c.host_scalars[kScalarCount + 2];
   if (pair_count == 0) return 0;
   c.pairs.ensure(pair_count);
-  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.members.p, c.coords.p, c.rank.p, c.cand_counts.p,
-                     c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus, c.stream);
+  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
+                     c.coords.p, c.rank.p, c.cand_counts.p, c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus,
+                     c.stream);
   c.pair_counts.ensure(pair_count + 1ull);
   c.pair_offsets.ensure(pair_count + 1ull);
   c.temp.ensure(scan_temp_words(pair_count + 1ull) + scan_temp_words(capacity) + sort_temp_words(n) + 64);
@@ -593,6 +643,7 @@ void fill_desc(Ctx& c, std::uint32_t row_count, float dt, const msb_growth_load_
   d.stall_load = growth.stall_load;
   d.tolerance = tolerance;
   d.max_iterations = max_iterations;
+  d.has_drift = c.has_drift ? 1u : 0u;
   // Copy only the problem part; the state part is reset in the graph.
   check(cudaMemcpyAsync(c.desc, &d, offsetof(SolveDesc, step), cudaMemcpyHostToDevice, c.stream), "desc");
 }
@@ -658,13 +709,17 @@ struct Attempt {
 Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, const msb_contact_parameters& cp,
                         const msb_constraint_contact_parameters& wp, bool probe, std::uint64_t& iterations) {
   const std::uint32_t n = c.n;
+  c.has_drift = false;  // the stepper's bodies carry no drift (flow drift is not supported)
   c.body_a.ensure(n);
   c.body_b.ensure(n);
   c.drift_a.ensure(n);
   c.drift_b.ensure(n);
+  mark(c, kPhaseRows);
   launch_make_bodies(n, c.state.view(), c.growth.p, c.fixed.p, c.initial.view(), p.drag,
                      {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream);
+  mark(c, kPhaseSearch);
   const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches);
+  mark(c, kPhaseRows);
   c.rows.count = 0;
   c.rows.ensure(std::max<std::uint32_t>(found, 1));
   reset_scalars(c);
@@ -682,7 +737,9 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   const float solve_tolerance = kSolveToleranceFraction * tolerance;
   Attempt attempt;
   for (std::uint32_t refinement = 0; refinement <= p.max_refinements; ++refinement) {
+    mark(c, kPhaseIncidence);
     build_system_incidence(c, c.rows.count);
+    mark(c, kPhaseSolve);
     std::uint32_t remaining = p.max_iterations;
     bool solved = false;
     if (probe && refinement == 0 && remaining > kRotationProbeIterations) {
@@ -707,6 +764,7 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
       if (full.status != MSB_SOLVE_CONVERGED) break;
     }
     // Move from the base geometry under the response of the solution.
+    mark(c, kPhaseMove);
     c.trial.ensure(n);
     reset_scalars(c);
     launch_move(n, c.base.view(), {c.resp_a.p, c.resp_b.p}, dt, c.trial.view(), c.scalars.p + kRotationBits,
@@ -716,7 +774,9 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
     if (c.host_scalars[kInvalid] != 0) break;
     launch_restore(n, c.trial.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
 
+    mark(c, kPhaseSearch);
     const std::uint32_t overlapping_candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
+    mark(c, kPhaseMove);
     c.flags.ensure(overlapping_candidates + 1ull);
     c.flag_offsets.ensure(overlapping_candidates + 1ull);
     reset_scalars(c);
@@ -740,6 +800,7 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
     }
     // Rows for the new overlaps, linearized at the trial geometry, with
     // offsets that the multipliers of the move predict (contact_dynamics.cpp:567-578).
+    mark(c, kPhaseRows);
     c.flagged.ensure(overlapping);
     launch_gather_flagged(c.found.p, overlapping_candidates, c.flags.p, c.flag_offsets.p, c.flagged.p, c.stream);
     const std::uint32_t base_row = c.rows.count;
@@ -864,6 +925,10 @@ void write_outputs(Ctx& c, msb_contact_dynamics_outputs* outputs, bool device_po
 void load_system(Ctx& c, const msb_contact_system& s, const float* multipliers) {
   validate_system(s);
   c.n = std::uint32_t(s.body_count);
+  c.has_drift = false;
+  for (std::uint64_t b = 0; b < s.body_count && !c.has_drift; ++b) {
+    for (float v : s.bodies[b].drift) c.has_drift = c.has_drift || v != 0.0f;
+  }
   const std::uint32_t rows = std::uint32_t(s.row_count);
   c.body_a.ensure(std::max<std::uint32_t>(c.n, 1));
   c.body_b.ensure(std::max<std::uint32_t>(c.n, 1));
@@ -969,6 +1034,7 @@ void msb_context_destroy(msb_context* context) {
   if (context == nullptr) return;
   cudaSetDevice(context->device);
   if (context->stream != nullptr) cudaStreamSynchronize(context->stream);
+  for (auto e : context->phase_events) cudaEventDestroy(e);
   context->graphs.clear();
   if (context->desc != nullptr) cudaFree(context->desc);
   if (context->host_scalars != nullptr) cudaFreeHost(context->host_scalars);
@@ -984,6 +1050,12 @@ const char* msb_last_error(const msb_context* context) {
 int msb_backend_info(const msb_context* context, char* device_name, size_t capacity) {
   if (context == nullptr || device_name == nullptr || capacity == 0) return MSB_ERR_INVALID_ARGUMENT;
   std::snprintf(device_name, capacity, "%s", context->device_name.c_str());
+  return MSB_OK;
+}
+
+int msb_last_step_phases(const msb_context* context, double* milliseconds, uint32_t capacity) {
+  if (context == nullptr || milliseconds == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  for (std::uint32_t k = 0; k < capacity && k < kPhaseEnd; ++k) milliseconds[k] = context->phase_ms[k];
   return MSB_OK;
 }
 
@@ -1186,12 +1258,17 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     validate_contact_parameters(cp);
     validate_constraint_parameters(wp);
     auto& c = *context;
+    c.phase_marks.clear();
+    mark(c, kPhaseLoad);
     load_cells(c, *cells, device_pointers);
     load_constraints(c, constraints, constraint_count);
     const auto outcome = advance(c, dt, *dynamics, cp, wp);
+    mark(c, kPhaseOutput);
     write_back(c, *cells, device_pointers);
     write_outputs(c, outputs, device_pointers);
+    mark(c, kPhaseEnd);
     sync(c);
+    collect_phases(c);
     *report = outcome.report;
   });
 }

@@ -111,17 +111,18 @@ void launch_grid_setup(const double* partials, std::uint32_t partial_count, std:
 void launch_bin_cells(GeometryView g, const double* bounds, const GridParams* grid,
                       std::uint32_t* cell_bucket, std::int64_t* cell_coords, std::uint32_t* bucket_counts,
                       cudaStream_t stream);
-void launch_scatter_cells(std::uint32_t cells, const std::uint32_t* cell_bucket,
-                          const std::uint32_t* bucket_starts, std::uint32_t* bucket_fill,
-                          std::uint32_t* members, cudaStream_t stream);
+// Cells in bucket order: FP32 outward-rounded boxes (slot in lo.w) and ids.
+void launch_scatter_cells(GeometryView g, const double* bounds, const std::uint32_t* cell_bucket,
+                          const std::uint32_t* bucket_starts, std::uint32_t* bucket_fill, float4* sorted_lo,
+                          float4* sorted_hi, std::uint64_t* sorted_id, cudaStream_t stream);
 // Candidate pairs: per cell, partners of higher id whose boxes overlap.
 // Counts go to counts[rank[cell]]; fill writes (first, second) slot pairs in
 // (first id, second id) order at offsets[rank[cell]].
 void launch_broad_phase(GeometryView g, const double* bounds, const GridParams* grid,
-                        const std::uint32_t* bucket_starts, const std::uint32_t* members,
-                        const std::int64_t* cell_coords, const std::uint32_t* rank,
-                        std::uint32_t* counts, const std::uint32_t* offsets, uint2* pairs,
-                        std::uint32_t* status, cudaStream_t stream);
+                        const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
+                        const std::uint64_t* sorted_id, const std::int64_t* cell_coords,
+                        const std::uint32_t* rank, std::uint32_t* counts, const std::uint32_t* offsets,
+                        uint2* pairs, std::uint32_t* status, cudaStream_t stream);
 // Narrow phase: per candidate, the number of contacts below the margin
 // (count pass, `touches` null) or the contacts themselves at offsets[pair].
 void launch_narrow_phase(GeometryView g, const uint2* pairs, std::uint64_t pair_count,

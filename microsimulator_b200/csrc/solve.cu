@@ -15,6 +15,7 @@
 //              of the CUDA graph that repeats the two passes.
 // The host launches the graph once per solve and reads the report once.
 
+#include <algorithm>
 #include <cfloat>
 #include <cstdint>
 
@@ -38,69 +39,127 @@ __device__ __forceinline__ float growth_factor(std::uint32_t law, float sensitiv
   return 1.0f;
 }
 
-// apply_mobility (cpu_contact_dynamics.cpp:40-53) plus drift.
-__device__ __forceinline__ void respond(const SolveDesc& d, std::uint32_t b, const float w[6], float load) {
-  const float4 ba = d.bodies.a[b];
-  const float4 bb = d.bodies.b[b];
-  const float4 da = d.bodies.drift_a[b];
-  const float4 db = d.bodies.drift_b[b];
+// apply_mobility (cpu_contact_dynamics.cpp:40-53) plus drift.  Without
+// drift the additions are of +0.0f, which leaves every value's bits as they
+// are, so the drift arrays are only read when the system has some.
+__device__ __forceinline__ void respond(const SolveDesc& d, std::uint32_t b, const float w[6], float load, float v[6],
+                                        float& rate) {
+  const float4 ba = __ldcs(&d.bodies.a[b]);
+  const float4 bb = __ldcs(&d.bodies.b[b]);
+  float4 da = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  float4 db = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  if (d.has_drift) {
+    da = d.bodies.drift_a[b];
+    db = d.bodies.drift_b[b];
+  }
   const F3 axis{ba.x, ba.y, ba.z};
   const F3 tq{w[3], w[4], w[5]};
   const float s = (bb.y - bb.x) * dot(axis, tq);
   const F3 ang = tq * bb.x + axis * s;
-  float v[6] = {w[0] * ba.w, w[1] * ba.w, w[2] * ba.w, ang.x, ang.y, ang.z};
+  v[0] = w[0] * ba.w;
+  v[1] = w[1] * ba.w;
+  v[2] = w[2] * ba.w;
+  v[3] = ang.x;
+  v[4] = ang.y;
+  v[5] = ang.z;
   v[0] += da.x;
   v[1] += da.y;
   v[2] += da.z;
   v[3] += db.x;
   v[4] += db.y;
   v[5] += db.z;
-  const float rate = bb.z > 0.0f ? bb.z * growth_factor(d.law, d.sensitivity, d.free_load, d.stall_load, load) : bb.z;
-  d.response.a[b] = make_float4(v[0], v[1], v[2], rate);
-  d.response.b[b] = make_float4(v[3], v[4], v[5], load);
+  rate = bb.z > 0.0f ? bb.z * growth_factor(d.law, d.sensitivity, d.free_load, d.stall_load, load) : bb.z;
 }
 
+// wrench_dot(jacobian, velocity) - lever * rate: one side's term of a row's
+// gap rate, as row_gap forms it (cpp/cpu/cpu_contact_dynamics.cpp:149-159).
+__device__ __forceinline__ float side_term(float4 ea, float4 eb, const float v[6], float rate) {
+  float r = 0.0f;
+  r += ea.x * v[0];
+  r += ea.y * v[1];
+  r += ea.z * v[2];
+  r += ea.w * v[3];
+  r += eb.x * v[4];
+  r += eb.y * v[5];
+  return r - eb.z * rate;
+}
+
+// Tuning constants of the BB passes: entries whose gathers one body-pass
+// thread keeps in flight together, and the minimum resident blocks per SM
+// the compiler must fit (which caps registers).
+#ifndef MSB_BODY_BATCH
+#define MSB_BODY_BATCH 4
+#endif
+#ifndef MSB_BODY_MIN_BLOCKS
+#define MSB_BODY_MIN_BLOCKS 4
+#endif
+#ifndef MSB_ROW_MIN_BLOCKS
+#define MSB_ROW_MIN_BLOCKS 1
+#endif
+constexpr int kBatch = MSB_BODY_BATCH;
+
+
+// One thread per body sums its rows' multipliers times their jacobians in
+// entry order, which is row order: the products and the order of the sums
+// are those of the reference's evaluate (cpp/cpu/cpu_contact_dynamics.cpp:116-146),
+// so a body's force, torque and load carry the reference's bits.  The entries
+// are read kBatch at a time and their multiplier gathers issued together, so
+// that each thread keeps several independent loads in flight.
 // mode 0 and 2 evaluate the multipliers as they are; mode 1 their projection.
 // `Tag` only names a second instance of the same code for the timing hook,
 // so that a profiler can select its launches apart from the solve graph's.
 template <int Tag>
-__global__ void __launch_bounds__(kSolveThreads) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
+__global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
   const SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
   const float alpha = d.step;
   const float* __restrict__ g = d.multipliers;
   const float* __restrict__ gap = d.gaps;
+  const std::uint32_t* __restrict__ offsets = d.incidence.offsets;
   for (std::uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < d.body_count; b += gridDim.x * blockDim.x) {
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float load = 0.0f;
-    const std::uint32_t end = d.incidence.offsets[b + 1];
-    for (std::uint32_t k = d.incidence.offsets[b]; k < end; ++k) {
-      const float4 ea = d.incidence.a[k];
-      const float4 eb = d.incidence.b[k];
-      const std::uint32_t row = __float_as_uint(eb.w);
-      const float m = mode == 1 ? smax(0.0f, g[row] - alpha * gap[row]) : g[row];
-      if (m == 0.0f) continue;
-      w[0] += m * ea.x;
-      w[1] += m * ea.y;
-      w[2] += m * ea.z;
-      w[3] += m * ea.w;
-      w[4] += m * eb.x;
-      w[5] += m * eb.y;
-      load += eb.z * m;
+    const std::uint32_t begin = offsets[b];
+    const std::uint32_t end = offsets[b + 1];
+    for (std::uint32_t k0 = begin; k0 < end; k0 += kBatch) {
+      float4 ea[kBatch], eb[kBatch];
+      float gv[kBatch], pv[kBatch];
+#pragma unroll
+      for (int t = 0; t < kBatch; ++t) {
+        if (k0 + t < end) {
+          ea[t] = __ldcs(&d.incidence.a[k0 + t]);
+          eb[t] = __ldcs(&d.incidence.b[k0 + t]);
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < kBatch; ++t) {
+        if (k0 + t < end) {
+          const std::uint32_t row = __float_as_uint(eb[t].w);
+          gv[t] = g[row];
+          pv[t] = mode == 1 ? gap[row] : 0.0f;
+        }
+      }
+#pragma unroll
+      for (int t = 0; t < kBatch; ++t) {
+        if (k0 + t < end) {
+          const float m = mode == 1 ? smax(0.0f, gv[t] - alpha * pv[t]) : gv[t];
+          if (m == 0.0f) continue;
+          w[0] += m * ea[t].x;
+          w[1] += m * ea[t].y;
+          w[2] += m * ea[t].z;
+          w[3] += m * ea[t].w;
+          w[4] += m * eb[t].x;
+          w[5] += m * eb[t].y;
+          load += eb[t].z * m;
+        }
+      }
     }
-    respond(d, b, w, load);
+    float v[6];
+    float rate;
+    respond(d, b, w, load, v, rate);
+    d.response.a[b] = make_float4(v[0], v[1], v[2], rate);
+    d.response.b[b] = make_float4(v[3], v[4], v[5], load);
   }
-}
-
-__device__ __forceinline__ float wrench_dot(float4 ja, float4 jb, float4 va, float4 vb) {
-  float r = 0.0f;
-  r += ja.x * va.x;
-  r += ja.y * va.y;
-  r += ja.z * va.z;
-  r += ja.w * vb.x;
-  r += jb.x * vb.y;
-  r += jb.y * vb.z;
-  return r;
 }
 
 __device__ __forceinline__ float row_residual(float m, float gap) {
@@ -118,7 +177,7 @@ __device__ __forceinline__ float next_step(float current, double ss, double sy, 
 // graph condition); mode 1: one projected step (sets the condition);
 // mode 2: gaps only.
 template <int Tag>
-__global__ void __launch_bounds__(kSolveThreads) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
+__global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
   SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
   const float alpha = d.step;
@@ -128,27 +187,32 @@ __global__ void __launch_bounds__(kSolveThreads) row_pass_kernel(SolveDesc* desc
   double ss = 0.0, sy = 0.0, yy = 0.0;
   float residual = 0.0f;
   bool finite = true;
+  // row_gap (cpp/cpu/cpu_contact_dynamics.cpp:149-159): each side's
+  // jacobian . velocity - lever * elongation rate, summed in that order.
+  const bool project = mode == 1;
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
     const float gi = g[i];
-    const float gpi = mode == 1 ? gap[i] : 0.0f;
-    const float m = mode == 1 ? smax(0.0f, gi - alpha * gpi) : gi;
-    const uint2 s = d.rows.slots[i];
-    const float4 ra = d.rows.a[i];
-    const float4 rb = d.rows.b[i];
+    const float gpi = project ? gap[i] : 0.0f;
+    const uint2 s = __ldcs(&d.rows.slots[i]);
+    const float4 ra = __ldcs(&d.rows.a[i]);
+    const float4 rb = __ldcs(&d.rows.b[i]);
+    const float4 rd = __ldcs(&d.rows.d[i]);
     const float4 va = d.response.a[s.x];
     const float4 vb = d.response.b[s.x];
-    float rate = wrench_dot(ra, rb, va, vb) - rb.z * va.w;
-    float4 rd = d.rows.d[i];
+    const float m = project ? smax(0.0f, gi - alpha * gpi) : gi;
+    const float v1[6] = {va.x, va.y, va.z, vb.x, vb.y, vb.z};
+    float rate = side_term(ra, rb, v1, va.w);
     if (s.y != kInvalidSlot) {
-      const float4 rc = d.rows.c[i];
+      const float4 rc = __ldcs(&d.rows.c[i]);
       const float4 wa = d.response.a[s.y];
       const float4 wb = d.response.b[s.y];
-      rate += wrench_dot(rc, rd, wa, wb) - rd.z * wa.w;
+      const float v2[6] = {wa.x, wa.y, wa.z, wb.x, wb.y, wb.z};
+      rate += side_term(rc, rd, v2, wa.w);
     }
     const float gn = rb.w + dt * rate + rd.w * m;
     residual = smax(residual, row_residual(m, gn));
     finite = finite && isfinite(gn);
-    if (mode == 1) {
+    if (project) {
       const double moved = double(m) - double(gi);
       const double change = double(gn) - double(gpi);
       ss += moved * moved;
@@ -358,9 +422,11 @@ int bits_for(std::uint32_t value) {
 
 }  // namespace
 
-void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
-                     std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
-                     cudaStream_t stream) {
+namespace {
+
+void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
+                    std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
+                    cudaStream_t stream) {
   cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
   if (row_count > 0) {
     incidence_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, body_count, keys,
@@ -371,13 +437,19 @@ void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body
   if (row_count == 0) return;
   const std::uint64_t n = 2ull * row_count;
   radix_sort_pairs(keys, values, n, bits_for(body_count), temp, stream);
-  // Wall rows have no second entry; those sorted to the end and are dropped
-  // by gathering only as many entries as the offsets count (read on device
-  // through the last offset would need a sync, so gather all 2R and let the
-  // offsets bound what the body pass reads).
+  // A constraint row has no second entry; its key sorts past every body and
+  // the offsets end before it, so gathering all 2R entries is harmless.
   incidence_gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(rows, values, std::uint32_t(n), incidence.a,
                                                                  incidence.b);
   count_launch();
+}
+
+}  // namespace
+
+void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
+                     std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
+                     cudaStream_t stream) {
+  incidence_pass(rows, row_count, body_count, incidence, keys, values, counts, temp, stream);
 }
 
 void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,
@@ -398,6 +470,14 @@ SolveGraph::~SolveGraph() {
 }
 
 int SolveGraph::create(SolveDesc* desc, int blocks, cudaStream_t stream) {
+  // At most one resident wave: a grid-stride pass whose blocks do not all
+  // fit at once leaves a partly empty second wave.
+  int device = 0, sms = kSmCount, body_active = 1, row_active = 1;
+  if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&body_active, body_pass_kernel<0>, kSolveThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&row_active, row_pass_kernel<0>, kSolveThreads, 0);
+  const int wave = sms * std::max(1, std::min(body_active, row_active));
+  blocks = std::max(1, std::min(blocks, wave));
   blocks_ = blocks;
   desc_ = desc;
   cudaError_t err = cudaGraphCreate(&graph_, 0);

@@ -66,6 +66,7 @@ struct SolveDesc {
   float stall_load;
   float tolerance;
   std::uint32_t max_iterations;
+  std::uint32_t has_drift;  // 0: every drift is zero and the drift arrays are not read
   // solver state
   float step;
   float residual;
