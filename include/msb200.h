@@ -362,6 +362,46 @@ int msb_advance_contact_dynamics_device(
 int msb_profile_iterations(msb_context* context, uint32_t iterations, float* body_ms, float* row_ms,
                            uint64_t* rows, uint64_t* bodies);
 
+/* One solve of the stepper: rows, iterations, final status and residual. */
+typedef struct msb_solve_record {
+  uint32_t rows;
+  uint32_t iterations;
+  uint32_t status;
+  float residual;
+} msb_solve_record;
+
+/* The solves of the last msb_advance_contact_dynamics(_device) call in the
+ * order they ran (probe, full solve, refinement re-solves, and those of
+ * rejected substeps).  *count receives their number; MSB_ERR_CAPACITY when
+ * it exceeds capacity (the first capacity records are written).  A
+ * diagnostic with no counterpart in the reference. */
+int msb_last_step_solves(const msb_context* context, msb_solve_record* records, uint32_t capacity,
+                         uint32_t* count);
+
+/* Warm starts of the stepper, extensions with no counterpart in the
+ * reference (whose stepper starts every step from zero multipliers and keeps
+ * no state between steps, contact_dynamics.cpp:725).  `mode` ORs flags:
+ *   0  none: the reference's semantics (the default);
+ *   1  carry: each step's first solve starts from the final contact forces of
+ *      the context's previous step, matched by the reference's substep keys
+ *      (first cell, partner, occurrence) and checked against cell ids, so a
+ *      divided cell's daughters start from zero;
+ *   2  guess: with a motion guess set for the step (msb_set_motion_guess),
+ *      the first solve of each substep starts from multipliers moved toward
+ *      the forces the guessed motion asks of each body (a least-squares step
+ *      along each body's rows).
+ * Only the multipliers a solve starts from change: the rows, the tolerance
+ * and the stepper's acceptance test are the reference's, and every solve
+ * converges to the same tolerance. */
+int msb_set_warm_start(msb_context* context, uint32_t mode);
+
+/* A motion guess for the next step of `context` only: guess[3 s + 0..2] =
+ * (dx, dy, dtheta) of cell slot s over `dt`, the displacement in the
+ * xy-plane and the turn about z (a monolayer).  Host memory; copied.  The
+ * next step fails with MSB_ERR_INVALID_ARGUMENT when its cell count differs
+ * from cell_count.  A null guess clears it. */
+int msb_set_motion_guess(msb_context* context, const float* guess, uint64_t cell_count, float dt);
+
 /* Device time of the last msb_advance_contact_dynamics(_device) call by
  * phase, measured with CUDA events on the context's stream, in
  * milliseconds: [0] upload, validation and id order; [1] contact searches;

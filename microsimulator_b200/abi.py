@@ -373,6 +373,9 @@ SIGNATURES = {
     ),
     "msb_launch_count": (c_uint64, [c_void_p]),
     "msb_last_step_phases": (c_int, [c_void_p, c_void_p, c_uint32]),
+    "msb_set_warm_start": (c_int, [c_void_p, c_uint32]),
+    "msb_set_motion_guess": (c_int, [c_void_p, c_void_p, c_uint64, c_float]),
+    "msb_last_step_solves": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "msb_solve_contact_forces_no_alloc": (
         c_int,
         [

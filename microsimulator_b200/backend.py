@@ -79,6 +79,42 @@ class B200Backend:
     def launch_count(self) -> int:
         return int(self._lib.msb_launch_count(self._handle))
 
+    WARM_START_ZERO = 0
+    WARM_START_CARRY = 1
+    WARM_START_GUESS = 2
+
+    def set_warm_start(self, mode: int) -> None:
+        """Flags: 0 the reference's semantics; 1 carry the previous step's
+        final forces; 2 move the start multipliers toward the forces that a
+        motion guess asks of each body."""
+        self._check(self._lib.msb_set_warm_start(self._handle, mode))
+
+    def set_motion_guess(self, guess, dt: float) -> None:
+        """(cells, 3) float32 displacement guess (dx, dy, dtheta) over dt for
+        the next step, or None to clear it."""
+        if guess is None:
+            self._check(self._lib.msb_set_motion_guess(self._handle, None, 0, c_float(dt)))
+            return
+        g = np.ascontiguousarray(guess, dtype=np.float32)
+        if g.ndim != 2 or g.shape[1] != 3:
+            raise ValueError("motion guess must have shape (cells, 3)")
+        self._check(self._lib.msb_set_motion_guess(self._handle, c_void_p(abi.ptr(g)), g.shape[0], c_float(dt)))
+
+    SOLVE_RECORD_DTYPE = np.dtype([("rows", "<u4"), ("iterations", "<u4"), ("status", "<u4"), ("residual", "<f4")])
+
+    def last_step_solves(self) -> np.ndarray:
+        """The solves of the last step in order: rows, iterations, status and
+        residual of each."""
+        count = ctypes.c_uint32(0)
+        out = np.zeros(64, dtype=self.SOLVE_RECORD_DTYPE)
+        status = self._lib.msb_last_step_solves(self._handle, c_void_p(abi.ptr(out)), len(out), ctypes.byref(count))
+        if status == abi.ERR_CAPACITY:
+            out = np.zeros(count.value, dtype=self.SOLVE_RECORD_DTYPE)
+            status = self._lib.msb_last_step_solves(self._handle, c_void_p(abi.ptr(out)), len(out),
+                                                    ctypes.byref(count))
+        self._check(status)
+        return out[: count.value].copy()
+
     PHASES = ("load", "search", "rows", "incidence", "solve", "move", "output")
 
     def last_step_phases(self) -> dict:

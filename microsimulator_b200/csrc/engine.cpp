@@ -167,6 +167,10 @@ constexpr std::uint32_t kRotationProbeIterations = 128;
 constexpr float kSolveToleranceFraction = 0.25f;
 constexpr float kLoadResolutionFraction = 0.1f;
 constexpr std::uint32_t kEasyRefinements = 2;
+// Warm-start flags (msb_set_warm_start).
+constexpr std::uint32_t kWarmCarry = 1;       // the previous step's final forces
+constexpr std::uint32_t kWarmGuess = 2;  // forces that a motion guess asks of each body
+constexpr std::uint32_t kWarmFlags = kWarmCarry | kWarmGuess;
 constexpr float kMaximumSubstepRotation = 0.5f;
 constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
 
@@ -322,6 +326,16 @@ struct msb_context {
   // the contact system
   msb::RowStore rows, memory;
   bool has_memory = false;
+  // Warm-start flags (msb_set_warm_start) and the cells of the memory.
+  std::uint32_t warm_start_mode = 0;
+  std::uint32_t memory_cells = 0;
+  msb::DBuf<std::uint64_t> memory_first_ids, memory_partner_ids;
+  // A per-cell motion guess for the next step (msb_set_motion_guess).
+  msb::DBuf<float4> guess, guess_a, guess_b;
+  msb::DBuf<float> guess_delta;
+  bool has_guess = false;
+  std::uint32_t guess_cells = 0;
+  float guess_dt = 0.0f;
   bool has_drift = false;  // a loaded system with some non-zero drift
   msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
   msb::DBuf<std::uint32_t> inc_offsets;
@@ -342,6 +356,7 @@ struct msb_context {
   // phase timing of the last step: events at phase boundaries
   std::vector<cudaEvent_t> phase_events;
   std::vector<int> phase_marks;
+  std::vector<msb_solve_record> solve_log;  // the solves of the last step, in order
   std::array<double, 8> phase_ms{};
 
   // outputs staging for host calls
@@ -692,6 +707,7 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
   sync(c);
   const SolveDesc& d = *c.host_desc;
   count_launch(int(2 * d.iterations));
+  c.solve_log.push_back({rows, d.iterations, d.status, d.residual});
   if (d.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
   return {d.status, d.iterations, d.residual};
 }
@@ -705,6 +721,73 @@ struct Attempt {
   std::uint32_t rows = 0;
   float max_overlap = 0.0f;
 };
+
+struct Overlaps {
+  std::uint32_t candidates = 0;   // touches in c.found
+  std::uint32_t overlapping = 0;  // flagged among them
+  float max_overlap = 0.0f;
+};
+
+// The overlap test of contact_dynamics.cpp:520-548 on the geometry in
+// c.state: touches at margin 0 into c.found, flags and their offsets.
+Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_constraint_contact_parameters& wp,
+                       const msb_contact_dynamics_parameters& p) {
+  Overlaps o;
+  mark(c, kPhaseSearch);
+  o.candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
+  mark(c, kPhaseMove);
+  c.flags.ensure(o.candidates + 1ull);
+  c.flag_offsets.ensure(o.candidates + 1ull);
+  reset_scalars(c);
+  check(cudaMemsetAsync(c.flags.p + o.candidates, 0, 4, c.stream), "memset");
+  launch_recheck(c.found.p, o.candidates, c.rows.keyed(), c.slack.p, p.wall_stiffness, p.contact_stiffness,
+                 c.flags.p, c.scalars.p + kOverlapBits, c.stream);
+  c.temp.ensure(scan_temp_words(o.candidates + 1ull) + 64);
+  exclusive_scan(c.flags.p, c.flag_offsets.p, o.candidates + 1ull, c.temp.p, c.stream);
+  check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 4, c.flag_offsets.p + o.candidates, 4,
+                        cudaMemcpyDeviceToHost, c.stream),
+        "read");
+  read_scalars(c);
+  o.overlapping = c.host_scalars[kScalarCount + 4];
+  o.max_overlap = bits_to_float(c.host_scalars[kOverlapBits]);
+  return o;
+}
+
+// Appends rows for the flagged touches, linearized at c.trial, with offsets
+// moved by -dt * the rate that `response` predicts.
+void append_overlap_rows(Ctx& c, const Overlaps& o, const ResponseArrays& response, const RowBuild& build) {
+  mark(c, kPhaseRows);
+  c.flagged.ensure(o.overlapping);
+  launch_gather_flagged(c.found.p, o.candidates, c.flags.p, c.flag_offsets.p, c.flagged.p, c.stream);
+  const std::uint32_t base_row = c.rows.count;
+  c.rows.grow(std::size_t(base_row) + o.overlapping, c.stream);
+  launch_make_rows(c.flagged.p, o.overlapping, c.trial.view(), build, &response, c.rows.arrays(), base_row,
+                   c.rows.partner.p, c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
+  c.rows.count = base_row + o.overlapping;
+  build_row_keys(c, c.rows);
+}
+
+// Start multipliers moved toward the forces a motion guess asks of each
+// body (guess_forces_kernel): the response of the current multipliers, the
+// guessed response, and one distribution pass per body.
+void guess_forces(Ctx& c, float dt, const msb_growth_load_response& growth) {
+  const std::uint32_t n = c.n;
+  const std::uint32_t rows = c.rows.count;
+  if (rows == 0) return;
+  mark(c, kPhaseRows);
+  c.resp_a.ensure(n);
+  c.resp_b.ensure(n);
+  c.guess_a.ensure(n);
+  c.guess_b.ensure(n);
+  c.guess_delta.ensure(rows);
+  fill_desc(c, rows, dt, growth, 0.0f, 0);
+  launch_evaluate(c.desc, std::max(1, grid_for(n, kSolveThreads)), false, c.stream);
+  const BodyArrays bodies{c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
+  const ResponseArrays guess{c.guess_a.p, c.guess_b.p};
+  launch_guess_response(n, c.guess.p, bodies, c.guess_dt, guess, c.stream);
+  launch_guess_forces(n, rows, {c.inc_offsets.p, c.inc_a.p, c.inc_b.p}, bodies, {c.resp_a.p, c.resp_b.p}, guess,
+                      c.rows.slots.p, c.guess_delta.p, c.rows.multipliers.p, c.stream);
+}
 
 Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, const msb_contact_parameters& cp,
                         const msb_constraint_contact_parameters& wp, bool probe, std::uint64_t& iterations) {
@@ -732,13 +815,15 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   launch_slack(c.scalars.p + kOverlapBits, tolerance, p.max_overlap_recovery, c.slack.p, c.stream);
   build_row_keys(c, c.rows);
   const KeyedLists memory = c.memory.keyed();
-  launch_warm_start(found, c.rows.slots.p, c.rows.keyed(), c.has_memory ? &memory : nullptr, c.rows.multipliers.p,
+  const MemoryCells cells{c.memory_first_ids.p, c.memory_partner_ids.p, c.ids.p, c.memory_cells};
+  launch_warm_start(found, c.rows.slots.p, c.rows.keyed(), c.has_memory ? &memory : nullptr, cells, c.rows.multipliers.p,
                     c.stream);
   const float solve_tolerance = kSolveToleranceFraction * tolerance;
   Attempt attempt;
   for (std::uint32_t refinement = 0; refinement <= p.max_refinements; ++refinement) {
     mark(c, kPhaseIncidence);
     build_system_incidence(c, c.rows.count);
+    if (refinement == 0 && (c.warm_start_mode & kWarmGuess) != 0 && c.has_guess) guess_forces(c, dt, p.growth);
     mark(c, kPhaseSolve);
     std::uint32_t remaining = p.max_iterations;
     bool solved = false;
@@ -774,42 +859,17 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
     if (c.host_scalars[kInvalid] != 0) break;
     launch_restore(n, c.trial.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
 
-    mark(c, kPhaseSearch);
-    const std::uint32_t overlapping_candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
-    mark(c, kPhaseMove);
-    c.flags.ensure(overlapping_candidates + 1ull);
-    c.flag_offsets.ensure(overlapping_candidates + 1ull);
-    reset_scalars(c);
-    check(cudaMemsetAsync(c.flags.p + overlapping_candidates, 0, 4, c.stream), "memset");
-    launch_recheck(c.found.p, overlapping_candidates, c.rows.keyed(), c.slack.p, p.wall_stiffness,
-                   p.contact_stiffness, c.flags.p, c.scalars.p + kOverlapBits, c.stream);
-    c.temp.ensure(scan_temp_words(overlapping_candidates + 1ull) + 64);
-    exclusive_scan(c.flags.p, c.flag_offsets.p, overlapping_candidates + 1ull, c.temp.p, c.stream);
-    check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 4, c.flag_offsets.p + overlapping_candidates, 4,
-                          cudaMemcpyDeviceToHost, c.stream),
-          "read");
-    read_scalars(c);
-    const std::uint32_t overlapping = c.host_scalars[kScalarCount + 4];
-    const float max_overlap = bits_to_float(c.host_scalars[kOverlapBits]);
-    if (overlapping == 0) {
+    const Overlaps found_overlaps = flag_overlaps(c, cp, wp, p);
+    if (found_overlaps.overlapping == 0) {
       attempt.accepted = true;
       attempt.refinements = refinement;
       attempt.rows = c.rows.count;
-      attempt.max_overlap = max_overlap;
+      attempt.max_overlap = found_overlaps.max_overlap;
       return attempt;
     }
     // Rows for the new overlaps, linearized at the trial geometry, with
     // offsets that the multipliers of the move predict (contact_dynamics.cpp:567-578).
-    mark(c, kPhaseRows);
-    c.flagged.ensure(overlapping);
-    launch_gather_flagged(c.found.p, overlapping_candidates, c.flags.p, c.flag_offsets.p, c.flagged.p, c.stream);
-    const std::uint32_t base_row = c.rows.count;
-    c.rows.grow(std::size_t(base_row) + overlapping, c.stream);
-    const ResponseArrays response{c.resp_a.p, c.resp_b.p};
-    launch_make_rows(c.flagged.p, overlapping, c.trial.view(), build, &response, c.rows.arrays(), base_row,
-                     c.rows.partner.p, c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
-    c.rows.count = base_row + overlapping;
-    build_row_keys(c, c.rows);
+    append_overlap_rows(c, found_overlaps, {c.resp_a.p, c.resp_b.p}, build);
   }
   launch_restore(n, c.base.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
   reset_scalars(c);
@@ -844,8 +904,10 @@ StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, 
   if (dt == 0.0f) return out;
   copy_geometry(c, c.initial, c.state);
   copy_geometry(c, c.base, c.state);
-  c.has_memory = false;
-  c.memory.count = 0;
+  if ((c.warm_start_mode & kWarmCarry) == 0) {
+    c.has_memory = false;
+    c.memory.count = 0;
+  }
 
   reset_scalars(c);
   launch_growth_bound(n, c.state.view(), c.growth.p, dt, c.scalars.p + kGrowthBits, c.stream);
@@ -886,6 +948,11 @@ StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, 
     out.report.max_overlap = attempt.max_overlap;
     std::swap(c.rows, c.memory);  // forces <- this substep's rows
     c.has_memory = true;
+    c.memory_cells = n;
+    c.memory_first_ids.ensure(std::max<std::uint32_t>(c.memory.count, 1));
+    c.memory_partner_ids.ensure(std::max<std::uint32_t>(c.memory.count, 1));
+    launch_memory_ids(c.memory.count, c.memory.slots.p, c.memory.partner.p, c.ids.p, c.memory_first_ids.p,
+                      c.memory_partner_ids.p, c.stream);
     if (attempt.refinements <= kEasyRefinements && 2.0f * attempt.rotation <= kPlannedSubstepRotation) {
       length = std::min(longest, length * 2.0f);
     }
@@ -1051,6 +1118,48 @@ int msb_backend_info(const msb_context* context, char* device_name, size_t capac
   if (context == nullptr || device_name == nullptr || capacity == 0) return MSB_ERR_INVALID_ARGUMENT;
   std::snprintf(device_name, capacity, "%s", context->device_name.c_str());
   return MSB_OK;
+}
+
+int msb_last_step_solves(const msb_context* context, msb_solve_record* records, uint32_t capacity,
+                         uint32_t* count) {
+  if (context == nullptr || count == nullptr || (capacity > 0 && records == nullptr)) return MSB_ERR_INVALID_ARGUMENT;
+  const auto& log = context->solve_log;
+  *count = std::uint32_t(log.size());
+  for (std::size_t k = 0; k < log.size() && k < capacity; ++k) records[k] = log[k];
+  return log.size() > capacity ? MSB_ERR_CAPACITY : MSB_OK;
+}
+
+int msb_set_warm_start(msb_context* context, uint32_t mode) {
+  if (context == nullptr || (mode & ~kWarmFlags) != 0) return MSB_ERR_INVALID_ARGUMENT;
+  context->warm_start_mode = mode;
+  if ((mode & kWarmCarry) == 0) context->has_memory = false;
+  return MSB_OK;
+}
+
+int msb_set_motion_guess(msb_context* context, const float* guess, uint64_t cell_count, float dt) {
+  if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  auto& c = *context;
+  return guarded(context, [&] {
+    c.has_guess = false;
+    if (guess == nullptr || cell_count == 0) return;
+    if (cell_count > std::numeric_limits<std::uint32_t>::max()) throw std::overflow_error("too many cells");
+    if (!(dt > 0.0f) || !std::isfinite(dt)) throw std::invalid_argument("motion guess dt must be positive");
+    std::vector<float4> packed(cell_count);
+    for (std::uint64_t s = 0; s < cell_count; ++s) {
+      const float x = guess[3 * s], y = guess[3 * s + 1], t = guess[3 * s + 2];
+      if (!std::isfinite(x) || !std::isfinite(y) || !std::isfinite(t)) {
+        throw std::invalid_argument("motion guess must be finite");
+      }
+      packed[s] = make_float4(x, y, t, 0.0f);
+    }
+    c.guess.ensure(cell_count);
+    check(cudaMemcpyAsync(c.guess.p, packed.data(), cell_count * sizeof(float4), cudaMemcpyHostToDevice, c.stream),
+          "copy guess");
+    sync(c);
+    c.guess_cells = std::uint32_t(cell_count);
+    c.guess_dt = dt;
+    c.has_guess = true;
+  });
 }
 
 int msb_last_step_phases(const msb_context* context, double* milliseconds, uint32_t capacity) {
@@ -1259,10 +1368,25 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     validate_constraint_parameters(wp);
     auto& c = *context;
     c.phase_marks.clear();
+    c.solve_log.clear();
     mark(c, kPhaseLoad);
     load_cells(c, *cells, device_pointers);
     load_constraints(c, constraints, constraint_count);
-    const auto outcome = advance(c, dt, *dynamics, cp, wp);
+    c.has_memory = c.has_memory && (c.warm_start_mode & kWarmCarry) != 0;
+    if (c.has_guess && c.guess_cells != c.n) {
+      c.has_guess = false;
+      throw std::invalid_argument("the motion guess covers " + std::to_string(c.guess_cells) +
+                                  " cells; the step has " + std::to_string(c.n));
+    }
+    StepOutcome outcome;
+    try {
+      outcome = advance(c, dt, *dynamics, cp, wp);
+    } catch (...) {
+      c.has_memory = false;  // forces of a step that did not complete
+      c.has_guess = false;
+      throw;
+    }
+    c.has_guess = false;  // a guess serves one step
     mark(c, kPhaseOutput);
     write_back(c, *cells, device_pointers);
     write_outputs(c, outputs, device_pointers);

@@ -146,10 +146,16 @@ __global__ void make_rows_kernel(const Touch* __restrict__ touches, std::uint32_
   }
 }
 
+// ForceMemory::force with the occurrence rule of advance_substep
+// (cpp/core/contact_dynamics.cpp:156-174,463-477): the force of the
+// occurrence-th remembered row with the same key, or zero.  A remembered row
+// counts only if its cells' ids match the current ones.
 __global__ void warm_start_kernel(std::uint32_t rows, const uint2* __restrict__ slots, KeyedLists current,
-                                  KeyedLists memory, int has_memory, float* __restrict__ multipliers) {
+                                  KeyedLists memory, MemoryCells cells, int has_memory,
+                                  float* __restrict__ multipliers) {
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const std::uint32_t first = slots[i].x;
+    const uint2 sl = slots[i];
+    const std::uint32_t first = sl.x;
     const std::uint64_t key = current.partner[i];
     std::uint32_t occurrence = 0;
     for (std::uint32_t k = current.offsets[first]; k < current.offsets[first + 1]; ++k) {
@@ -158,10 +164,12 @@ __global__ void warm_start_kernel(std::uint32_t rows, const uint2* __restrict__ 
       occurrence += current.partner[r] == key ? 1u : 0u;
     }
     float force = 0.0f;
-    if (has_memory) {
+    if (has_memory && first < cells.cells) {
+      const std::uint64_t first_id = cells.ids[first];
+      const std::uint64_t partner_id = sl.y == kInvalidSlot ? key : cells.ids[sl.y];
       for (std::uint32_t k = memory.offsets[first]; k < memory.offsets[first + 1]; ++k) {
         const std::uint32_t r = memory.rows[k];
-        if (memory.partner[r] == key) {
+        if (memory.partner[r] == key && cells.first_ids[r] == first_id && cells.partner_ids[r] == partner_id) {
           if (occurrence == 0) {
             force = memory.multipliers[r];
             break;
@@ -171,6 +179,16 @@ __global__ void warm_start_kernel(std::uint32_t rows, const uint2* __restrict__ 
       }
     }
     multipliers[i] = force;
+  }
+}
+
+__global__ void memory_ids_kernel(std::uint32_t rows, const uint2* __restrict__ slots,
+                                  const std::uint64_t* __restrict__ partner, const std::uint64_t* __restrict__ ids,
+                                  std::uint64_t* __restrict__ first_ids, std::uint64_t* __restrict__ partner_ids) {
+  for (std::uint32_t r = blockIdx.x * blockDim.x + threadIdx.x; r < rows; r += gridDim.x * blockDim.x) {
+    const uint2 sl = slots[r];
+    first_ids[r] = ids[sl.x];
+    partner_ids[r] = sl.y == kInvalidSlot ? partner[r] : ids[sl.y];
   }
 }
 
@@ -218,6 +236,76 @@ __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArray
     if (!finite3(pos) || !finite3(dir) || !isfinite(len) || len < 0.0f) atomicExch(invalid, 1u);
     trial.pos_len[s] = make_float4(pos.x, pos.y, pos.z, len);
     trial.dir_rad[s] = make_float4(dir.x, dir.y, dir.z, dr.w);
+  }
+}
+
+__global__ void guess_response_kernel(std::uint32_t n, const float4* __restrict__ guess, BodyArrays bodies,
+                                      float inverse_dt, ResponseArrays out) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float4 g = guess[s];
+    const float rate = bodies.b[s].z;
+    out.a[s] = make_float4(g.x * inverse_dt, g.y * inverse_dt, 0.0f, rate);
+    out.b[s] = make_float4(0.0f, 0.0f, g.z * inverse_dt, 0.0f);
+  }
+}
+
+// The wrench that moves body b by v (the inverse of apply_mobility,
+// cpp/cpu/cpu_contact_dynamics.cpp:40-53); zero for a body that cannot move.
+__device__ __forceinline__ void wrench_for(float4 ba, float4 bb, const float v[6], float w[6]) {
+  const bool moves = ba.w > 0.0f && bb.x > 0.0f && bb.y > 0.0f;
+  for (int k = 0; k < 6; ++k) w[k] = 0.0f;
+  if (!moves) return;
+  const F3 axis{ba.x, ba.y, ba.z};
+  const F3 ang{v[3], v[4], v[5]};
+  const float s = (1.0f / bb.y - 1.0f / bb.x) * dot(axis, ang);
+  const F3 tq = ang * (1.0f / bb.x) + axis * s;
+  w[0] = v[0] / ba.w;
+  w[1] = v[1] / ba.w;
+  w[2] = v[2] / ba.w;
+  w[3] = tq.x;
+  w[4] = tq.y;
+  w[5] = tq.z;
+}
+
+__global__ void guess_forces_body_kernel(std::uint32_t n, IncidenceArrays inc, BodyArrays bodies,
+                                         ResponseArrays current, ResponseArrays guess, const uint2* __restrict__ slots,
+                                         float* __restrict__ delta) {
+  for (std::uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < n; b += gridDim.x * blockDim.x) {
+    const float4 ca = current.a[b], cb = current.b[b], ga = guess.a[b], gb = guess.b[b];
+    const float dv[6] = {ga.x - ca.x, ga.y - ca.y, ga.z - ca.z, gb.x - cb.x, gb.y - cb.y, gb.z - cb.z};
+    float w[6];
+    wrench_for(bodies.a[b], bodies.b[b], dv, w);
+    const std::uint32_t begin = inc.offsets[b], end = inc.offsets[b + 1];
+    float uu = 0.0f;
+    float r[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    for (std::uint32_t k = begin; k < end; ++k) {
+      const float4 ea = inc.a[k], eb = inc.b[k];
+      const float j[6] = {ea.x, ea.y, ea.z, ea.w, eb.x, eb.y};
+      float u = 0.0f;
+      for (int q = 0; q < 6; ++q) u += j[q] * w[q];
+      uu += u * u;
+      for (int q = 0; q < 6; ++q) r[q] += u * j[q];
+    }
+    float rr = 0.0f;
+    for (int q = 0; q < 6; ++q) rr += r[q] * r[q];
+    if (!(rr > 0.0f) || !(uu > 0.0f)) continue;
+    const float alpha = uu / rr;
+    for (std::uint32_t k = begin; k < end; ++k) {
+      const float4 ea = inc.a[k], eb = inc.b[k];
+      const float u = ea.x * w[0] + ea.y * w[1] + ea.z * w[2] + ea.w * w[3] + eb.x * w[4] + eb.y * w[5];
+      const std::uint32_t row = __float_as_uint(eb.w);
+      const float share = slots[row].y == kInvalidSlot ? 1.0f : 0.5f;
+      // At most two additions onto zero per row: the sum does not depend on their order.
+      atomicAdd(&delta[row], share * alpha * u);
+    }
+  }
+}
+
+__global__ void guess_forces_row_kernel(std::uint32_t rows, const float* __restrict__ delta,
+                                        float* __restrict__ multipliers) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const float m = multipliers[i] + delta[i];
+    multipliers[i] = isfinite(m) ? smax(0.0f, m) : multipliers[i];
   }
 }
 
@@ -390,11 +478,19 @@ void launch_make_rows(const Touch* touches, std::uint32_t count, GeometryBuffers
 }
 
 void launch_warm_start(std::uint32_t rows, const uint2* slots, KeyedLists current, const KeyedLists* memory,
-                       float* multipliers, cudaStream_t stream) {
+                       MemoryCells cells, float* multipliers, cudaStream_t stream) {
   if (rows == 0) return;
   const KeyedLists none{nullptr, nullptr, nullptr, nullptr};
   warm_start_kernel<<<grid_for(rows, kThreads), kThreads, 0, stream>>>(
-      rows, slots, current, memory != nullptr ? *memory : none, memory != nullptr ? 1 : 0, multipliers);
+      rows, slots, current, memory != nullptr ? *memory : none, cells, memory != nullptr ? 1 : 0, multipliers);
+  count_launch();
+}
+
+void launch_memory_ids(std::uint32_t rows, const uint2* slots, const std::uint64_t* partner, const std::uint64_t* ids,
+                       std::uint64_t* first_ids, std::uint64_t* partner_ids, cudaStream_t stream) {
+  if (rows == 0) return;
+  memory_ids_kernel<<<grid_for(rows, kThreads), kThreads, 0, stream>>>(rows, slots, partner, ids, first_ids,
+                                                                        partner_ids);
   count_launch();
 }
 
@@ -403,6 +499,25 @@ void launch_move(std::uint32_t n, GeometryBuffers base, ResponseArrays response,
   if (n == 0) return;
   move_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, base, response, dt, trial, rotation_bits, invalid,
                                                                status);
+  count_launch();
+}
+
+void launch_guess_response(std::uint32_t n, const float4* guess, BodyArrays bodies, float step_dt,
+                           ResponseArrays out, cudaStream_t stream) {
+  if (n == 0) return;
+  guess_response_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, guess, bodies, 1.0f / step_dt, out);
+  count_launch();
+}
+
+void launch_guess_forces(std::uint32_t n, std::uint32_t rows, IncidenceArrays incidence, BodyArrays bodies,
+                         ResponseArrays current, ResponseArrays guess, const uint2* slots, float* delta,
+                         float* multipliers, cudaStream_t stream) {
+  if (n == 0 || rows == 0) return;
+  cudaMemsetAsync(delta, 0, rows * sizeof(float), stream);
+  guess_forces_body_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, incidence, bodies, current, guess,
+                                                                          slots, delta);
+  count_launch();
+  guess_forces_row_kernel<<<grid_for(rows, kThreads), kThreads, 0, stream>>>(rows, delta, multipliers);
   count_launch();
 }
 

@@ -51,13 +51,41 @@ struct KeyedLists {
   const std::uint64_t* partner;
   const float* multipliers;
 };
+// The cells a remembered row belongs to, so that forces carried from one
+// step to the next never reach a slot that now holds another cell (a
+// divided parent's slot holds its first daughter).
+struct MemoryCells {
+  const std::uint64_t* first_ids;    // per remembered row: its first cell's id
+  const std::uint64_t* partner_ids;  // per remembered row: its second cell's id, or its wall key
+  const std::uint64_t* ids;          // the current ids, by slot
+  std::uint32_t cells;               // cells when the memory was made; later slots are new
+};
 void launch_warm_start(std::uint32_t rows, const uint2* slots, KeyedLists current, const KeyedLists* memory,
-                       float* multipliers, cudaStream_t stream);
+                       MemoryCells cells, float* multipliers, cudaStream_t stream);
+// Records the cell ids of remembered rows (see MemoryCells).
+void launch_memory_ids(std::uint32_t rows, const uint2* slots, const std::uint64_t* partner,
+                       const std::uint64_t* ids, std::uint64_t* first_ids, std::uint64_t* partner_ids,
+                       cudaStream_t stream);
 
 // moved (contact_dynamics.cpp:311-356): trial geometry, largest rotation
 // (bits) and a validity flag (0 = valid).
 void launch_move(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt, GeometryBuffers trial,
                  std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream);
+// A response from a per-cell motion guess: guess[s] = (dx, dy, dtheta, _),
+// the displacement in the xy-plane and the turn about z over `step_dt`;
+// the elongation rate is each body's nominal rate.
+void launch_guess_response(std::uint32_t n, const float4* guess, BodyArrays bodies, float step_dt,
+                           ResponseArrays out, cudaStream_t stream);
+// Moves start multipliers toward the forces a motion guess asks of each
+// body.  Per body b: the wrench w = M^-1 (guessed - current response) that
+// the guess lacks, and the least-squares step along its rows' jacobians
+// (delta_k = alpha j_k.w, alpha = sum (j_k.w)^2 / |sum (j_k.w) j_k|^2); a
+// row takes the mean of its bodies' steps (a wall row its one body's), and
+// multipliers become max(0, multipliers + delta).  `delta` is scratch of
+// `rows` floats.
+void launch_guess_forces(std::uint32_t n, std::uint32_t rows, IncidenceArrays incidence, BodyArrays bodies,
+                         ResponseArrays current, ResponseArrays guess, const uint2* slots, float* delta,
+                         float* multipliers, cudaStream_t stream);
 // Largest angle of a response (infinity when one is not finite).
 void launch_largest_rotation(std::uint32_t n, ResponseArrays response, float dt, std::uint32_t* rotation_bits,
                              cudaStream_t stream);
