@@ -389,7 +389,10 @@ int msb_last_step_solves(const msb_context* context, msb_solve_record* records, 
  *   2  guess: with a motion guess set for the step (msb_set_motion_guess),
  *      the first solve of each substep starts from multipliers moved toward
  *      the forces the guessed motion asks of each body (a least-squares step
- *      along each body's rows).
+ *      along each body's rows);
+ *   4  learned: the warm-start network (msb_set_warm_start_network) makes
+ *      the motion guess of every step from the cells' neighbour features,
+ *      used as flag 2 uses a guess.
  * Only the multipliers a solve starts from change: the rows, the tolerance
  * and the stepper's acceptance test are the reference's, and every solve
  * converges to the same tolerance. */
@@ -402,12 +405,64 @@ int msb_set_warm_start(msb_context* context, uint32_t mode);
  * from cell_count.  A null guess clears it. */
 int msb_set_motion_guess(msb_context* context, const float* guess, uint64_t cell_count, float dt);
 
+/* ---- The warm-start network (no counterpart in the reference) ----------
+ *
+ * A per-cell MLP that guesses each cell's displacement over a step from its
+ * neighbourhood: 81 features (for each of the 16 nearest centres, the offset
+ * in the cell's frame along and across its axis over 5 um, the cosine and
+ * sine of the neighbour's orientation relative to the cell's with axis signs
+ * aligned, and the neighbour's length over 3 um; then the cell's own length
+ * over 3 um), zero-padded to 96; three hidden layers of 128 with GELU
+ * (the error-function form); 3 outputs, the normalized displacement along
+ * the axis, across it, and the turn.  Weights and activations are bf16, sums
+ * fp32, on the tensor cores.  All pointers below are device memory. */
+enum {
+  MSB_MLP_INPUT = 96,
+  MSB_MLP_HIDDEN = 128,
+  MSB_MLP_OUTPUTS = 3,
+  /* bf16 weights, row-major (out, in): W0 128x96 | W1 128x128 | W2 128x128 | W3 8x128 (rows 3..7 zero) */
+  MSB_MLP_WEIGHTS = 45056,
+  /* fp32 biases: b0 128 | b1 128 | b2 128 | b3 8 */
+  MSB_MLP_BIASES = 392,
+  /* fp32 parameters for training: the weights' layout followed by the biases' */
+  MSB_MLP_PARAMETERS = 45448
+};
+
+/* Features of the cells (device arrays in msb_cell_arrays) into `features`,
+ * count x MSB_MLP_INPUT bf16 (uint16 bits).  The 16 nearest centres are
+ * searched in the 3 x 3 bins of 6 um around each cell (exact whenever the
+ * 16th lies within 6 um); missing neighbours give zero features. */
+int msb_cell_features(msb_context* context, const msb_cell_arrays* cells, uint16_t* features);
+/* Bytes of the activations msb_mlp_forward keeps for msb_mlp_backward, and
+ * of msb_mlp_backward's scratch, for `rows` rows. */
+uint64_t msb_mlp_activation_bytes(uint64_t rows);
+uint64_t msb_mlp_backward_scratch_bytes(uint64_t rows);
+/* outputs (rows x 3 fp32) of the network on `features`; with a non-null
+ * `activations` buffer, keeps what msb_mlp_backward needs.  `stream` is a
+ * cudaStream_t (null: the default stream). */
+int msb_mlp_forward(const uint16_t* weights, const float* biases, const uint16_t* features, uint64_t rows,
+                    float* outputs, void* activations, void* stream);
+/* Gradients (MSB_MLP_PARAMETERS fp32, the parameters' layout) of a loss
+ * whose gradient with respect to the outputs is output_grad (rows x 3). */
+int msb_mlp_backward(const uint16_t* weights, const uint16_t* features, uint64_t rows, const void* activations,
+                     const float* output_grad, float* grads, void* scratch, void* stream);
+/* One Adam step (bias-corrected, step >= 1) on the fp32 parameters; writes
+ * the bf16 weights and fp32 biases the network reads. */
+int msb_mlp_adam(float* params, const float* grads, float* m, float* v, uint32_t step, float lr, float beta1,
+                 float beta2, float epsilon, uint16_t* weights, float* biases, void* stream);
+/* Gives the context a network (weights and biases copied; host or device
+ * memory) and the scales of its three outputs (um, um, rad), for warm-start
+ * flag 4.  A null `weights` removes it. */
+int msb_set_warm_start_network(msb_context* context, const uint16_t* weights, const float* biases,
+                               const float* scale);
+
 /* Device time of the last msb_advance_contact_dynamics(_device) call by
  * phase, measured with CUDA events on the context's stream, in
  * milliseconds: [0] upload, validation and id order; [1] contact searches;
  * [2] bodies, rows, keys and warm start; [3] incidence builds; [4] BB solves;
- * [5] moves and overlap re-checks; [6] outputs and download.  Writes
- * min(capacity, 7) values.  A measurement aid with no counterpart in the
+ * [5] moves and overlap re-checks; [6] outputs and download; [7] the
+ * learned warm start's features and network.  Writes min(capacity, 8)
+ * values.  A measurement aid with no counterpart in the
  * reference. */
 int msb_last_step_phases(const msb_context* context, double* milliseconds, uint32_t capacity);
 

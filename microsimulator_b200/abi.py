@@ -374,6 +374,14 @@ SIGNATURES = {
     "msb_launch_count": (c_uint64, [c_void_p]),
     "msb_last_step_phases": (c_int, [c_void_p, c_void_p, c_uint32]),
     "msb_set_warm_start": (c_int, [c_void_p, c_uint32]),
+    "msb_cell_features": (c_int, [c_void_p, c_void_p, c_void_p]),
+    "msb_mlp_activation_bytes": (c_uint64, [c_uint64]),
+    "msb_mlp_backward_scratch_bytes": (c_uint64, [c_uint64]),
+    "msb_mlp_forward": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_void_p]),
+    "msb_mlp_backward": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "msb_mlp_adam": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_float, c_float, c_float, c_float,
+                             c_void_p, c_void_p, c_void_p]),
+    "msb_set_warm_start_network": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "msb_set_motion_guess": (c_int, [c_void_p, c_void_p, c_uint64, c_float]),
     "msb_last_step_solves": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "msb_solve_contact_forces_no_alloc": (

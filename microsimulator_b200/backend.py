@@ -82,11 +82,13 @@ class B200Backend:
     WARM_START_ZERO = 0
     WARM_START_CARRY = 1
     WARM_START_GUESS = 2
+    WARM_START_LEARNED = 4
 
     def set_warm_start(self, mode: int) -> None:
         """Flags: 0 the reference's semantics; 1 carry the previous step's
         final forces; 2 move the start multipliers toward the forces that a
-        motion guess asks of each body."""
+        motion guess asks of each body; 4 let the warm-start network make
+        that guess each step (see learned.py)."""
         self._check(self._lib.msb_set_warm_start(self._handle, mode))
 
     def set_motion_guess(self, guess, dt: float) -> None:
@@ -115,7 +117,7 @@ class B200Backend:
         self._check(status)
         return out[: count.value].copy()
 
-    PHASES = ("load", "search", "rows", "incidence", "solve", "move", "output")
+    PHASES = ("load", "search", "rows", "incidence", "solve", "move", "output", "guess")
 
     def last_step_phases(self) -> dict:
         """Device milliseconds of the last step by phase (CUDA events)."""

@@ -28,6 +28,7 @@
 #include "kernels.h"
 #include "solve.h"
 #include "step.h"
+#include "mlp.h"
 
 namespace msb {
 
@@ -169,8 +170,9 @@ constexpr float kLoadResolutionFraction = 0.1f;
 constexpr std::uint32_t kEasyRefinements = 2;
 // Warm-start flags (msb_set_warm_start).
 constexpr std::uint32_t kWarmCarry = 1;       // the previous step's final forces
-constexpr std::uint32_t kWarmGuess = 2;  // forces that a motion guess asks of each body
-constexpr std::uint32_t kWarmFlags = kWarmCarry | kWarmGuess;
+constexpr std::uint32_t kWarmGuess = 2;    // forces that a motion guess asks of each body
+constexpr std::uint32_t kWarmLearned = 4;  // the warm-start network makes the motion guess
+constexpr std::uint32_t kWarmFlags = kWarmCarry | kWarmGuess | kWarmLearned;
 constexpr float kMaximumSubstepRotation = 0.5f;
 constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
 
@@ -333,6 +335,14 @@ struct msb_context {
   // A per-cell motion guess for the next step (msb_set_motion_guess).
   msb::DBuf<float4> guess, guess_a, guess_b;
   msb::DBuf<float> guess_delta;
+  // The warm-start network (msb_set_warm_start_network) and its buffers.
+  msb::DBuf<std::uint16_t> net_weights;
+  msb::DBuf<float> net_biases;
+  float net_scale[3] = {1.0f, 1.0f, 1.0f};
+  bool has_network = false;
+  msb::DBuf<std::uint16_t> features;
+  msb::DBuf<float> net_outputs;
+  msb::DBuf<std::uint32_t> knn_keys, knn_values, knn_counts, knn_offsets, knn_bounds;
   bool has_guess = false;
   std::uint32_t guess_cells = 0;
   float guess_dt = 0.0f;
@@ -378,7 +388,8 @@ enum Phase : int {
   kPhaseSolve = 4,      // the BB solves
   kPhaseMove = 5,       // move, restore, overlap re-check
   kPhaseOutput = 6,     // outputs and download
-  kPhaseEnd = 7
+  kPhaseGuess = 7,      // neighbour features and the warm-start network
+  kPhaseEnd = 8
 };
 
 // Records an event on the stream where `phase` begins (the previous phase ends).
@@ -767,6 +778,68 @@ void append_overlap_rows(Ctx& c, const Overlaps& o, const ResponseArrays& respon
   build_row_keys(c, c.rows);
 }
 
+float from_ordered(std::uint32_t u) {
+  const std::uint32_t b = (u & 0x80000000u) != 0 ? (u & 0x7FFFFFFFu) : ~u;
+  float f;
+  std::memcpy(&f, &b, 4);
+  return f;
+}
+
+// Neighbour features of the cells in `geometry` into c.features: a grid of
+// mlp::kBinSide bins over the centres (wider when the centres are sparse, so
+// that bins never outnumber four per cell), cells counting-sorted by bin.
+void compute_features(Ctx& c, GeometryBuffers geometry) {
+  const std::uint32_t n = c.n;
+  c.features.ensure(std::size_t(std::max<std::uint32_t>(n, 1)) * mlp::kInput);
+  if (n == 0) return;
+  c.knn_bounds.ensure(4);
+  mlp::launch_centre_bounds(n, geometry.pos_len, c.knn_bounds.p, c.stream);
+  check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 8, c.knn_bounds.p, 16, cudaMemcpyDeviceToHost, c.stream),
+        "read bounds");
+  sync(c);
+  const float x0 = from_ordered(c.host_scalars[kScalarCount + 8]);
+  const float y0 = from_ordered(c.host_scalars[kScalarCount + 9]);
+  const float x1 = from_ordered(c.host_scalars[kScalarCount + 10]);
+  const float y1 = from_ordered(c.host_scalars[kScalarCount + 11]);
+  if (!std::isfinite(x0) || !std::isfinite(y0) || !std::isfinite(x1) || !std::isfinite(y1)) {
+    throw std::invalid_argument("cell centres must be finite");
+  }
+  double side = mlp::kBinSide;
+  const double area = (double(x1 - x0) + side) * (double(y1 - y0) + side);
+  const double max_bins = 4.0 * n + 64.0;
+  if (area / (side * side) > max_bins) side = std::sqrt(area / max_bins) * 1.01;
+  const auto nx = std::uint32_t(std::floor(double(x1 - x0) / side)) + 1;
+  const auto ny = std::uint32_t(std::floor(double(y1 - y0) / side)) + 1;
+  const std::uint32_t bins = nx * ny;
+  c.knn_keys.ensure(n);
+  c.knn_values.ensure(n);
+  c.knn_counts.ensure(bins + 1ull);
+  c.knn_offsets.ensure(bins + 1ull);
+  c.temp.ensure(sort_temp_words(n) + scan_temp_words(bins + 1ull) + 64);
+  check(cudaMemsetAsync(c.knn_counts.p, 0, (bins + 1ull) * 4, c.stream), "memset");
+  mlp::Grid grid{x0, y0, float(1.0 / side), nx, ny, c.knn_offsets.p, c.knn_values.p};
+  mlp::launch_bin_keys(n, geometry.pos_len, grid, c.knn_keys.p, c.knn_values.p, c.knn_counts.p, c.stream);
+  exclusive_scan(c.knn_counts.p, c.knn_offsets.p, bins + 1ull, c.temp.p, c.stream);
+  const int bits = std::max(1, int(std::bit_width(bins)));
+  radix_sort_pairs(c.knn_keys.p, c.knn_values.p, n, bits, c.temp.p, c.stream);
+  mlp::launch_features(n, geometry.pos_len, geometry.dir_rad, grid, c.features.p, c.stream);
+}
+
+// The network's motion guess for the step from the geometry in c.state.
+void learned_guess(Ctx& c, float dt) {
+  const std::uint32_t n = c.n;
+  mark(c, kPhaseGuess);
+  compute_features(c, c.state.view());
+  c.net_outputs.ensure(3ull * std::max<std::uint32_t>(n, 1));
+  c.guess.ensure(std::max<std::uint32_t>(n, 1));
+  mlp::launch_forward(c.net_weights.p, c.net_biases.p, c.features.p, n, c.net_outputs.p, nullptr, c.stream);
+  mlp::launch_outputs_to_guess(n, c.net_outputs.p, c.net_scale, c.state.dir_rad.p, c.guess.p, c.stream);
+  check(cudaGetLastError(), "warm-start network");
+  c.guess_cells = n;
+  c.guess_dt = dt;
+  c.has_guess = true;
+}
+
 // Start multipliers moved toward the forces a motion guess asks of each
 // body (guess_forces_kernel): the response of the current multipliers, the
 // guessed response, and one distribution pass per body.
@@ -823,7 +896,9 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   for (std::uint32_t refinement = 0; refinement <= p.max_refinements; ++refinement) {
     mark(c, kPhaseIncidence);
     build_system_incidence(c, c.rows.count);
-    if (refinement == 0 && (c.warm_start_mode & kWarmGuess) != 0 && c.has_guess) guess_forces(c, dt, p.growth);
+    if (refinement == 0 && (c.warm_start_mode & (kWarmGuess | kWarmLearned)) != 0 && c.has_guess) {
+      guess_forces(c, dt, p.growth);
+    }
     mark(c, kPhaseSolve);
     std::uint32_t remaining = p.max_iterations;
     bool solved = false;
@@ -904,6 +979,10 @@ StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, 
   if (dt == 0.0f) return out;
   copy_geometry(c, c.initial, c.state);
   copy_geometry(c, c.base, c.state);
+  if ((c.warm_start_mode & kWarmLearned) != 0) {
+    if (!c.has_network) throw std::invalid_argument("the learned warm start needs a network (msb_set_warm_start_network)");
+    learned_guess(c, dt);
+  }
   if ((c.warm_start_mode & kWarmCarry) == 0) {
     c.has_memory = false;
     c.memory.count = 0;
@@ -1134,6 +1213,87 @@ int msb_set_warm_start(msb_context* context, uint32_t mode) {
   context->warm_start_mode = mode;
   if ((mode & kWarmCarry) == 0) context->has_memory = false;
   return MSB_OK;
+}
+
+uint64_t msb_mlp_activation_bytes(uint64_t rows) { return mlp::activation_bytes(rows); }
+uint64_t msb_mlp_backward_scratch_bytes(uint64_t rows) { return mlp::backward_scratch_bytes(rows); }
+
+namespace {
+int cuda_status(cudaError_t e) { return e == cudaSuccess ? MSB_OK : MSB_ERR_CUDA; }
+}  // namespace
+
+int msb_mlp_forward(const uint16_t* weights, const float* biases, const uint16_t* features, uint64_t rows,
+                    float* outputs, void* activations, void* stream) {
+  if (rows > std::numeric_limits<std::uint32_t>::max() / 2) return MSB_ERR_OVERFLOW;
+  if (rows > 0 && (weights == nullptr || biases == nullptr || features == nullptr || outputs == nullptr)) {
+    return MSB_ERR_INVALID_ARGUMENT;
+  }
+  mlp::launch_forward(weights, biases, features, std::uint32_t(rows), outputs, activations,
+                      static_cast<cudaStream_t>(stream));
+  return cuda_status(cudaGetLastError());
+}
+
+int msb_mlp_backward(const uint16_t* weights, const uint16_t* features, uint64_t rows, const void* activations,
+                     const float* output_grad, float* grads, void* scratch, void* stream) {
+  if (rows > std::numeric_limits<std::uint32_t>::max() / 2) return MSB_ERR_OVERFLOW;
+  if (grads == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  if (rows > 0 && (weights == nullptr || features == nullptr || activations == nullptr || output_grad == nullptr ||
+                   scratch == nullptr)) {
+    return MSB_ERR_INVALID_ARGUMENT;
+  }
+  mlp::launch_backward(weights, features, std::uint32_t(rows), activations, output_grad, grads, scratch,
+                       static_cast<cudaStream_t>(stream));
+  return cuda_status(cudaGetLastError());
+}
+
+int msb_mlp_adam(float* params, const float* grads, float* m, float* v, uint32_t step, float lr, float beta1,
+                 float beta2, float epsilon, uint16_t* weights, float* biases, void* stream) {
+  if (params == nullptr || grads == nullptr || m == nullptr || v == nullptr || weights == nullptr ||
+      biases == nullptr || step == 0 || !(lr > 0.0f) || !(beta1 >= 0.0f && beta1 < 1.0f) ||
+      !(beta2 >= 0.0f && beta2 < 1.0f) || !(epsilon > 0.0f)) {
+    return MSB_ERR_INVALID_ARGUMENT;
+  }
+  mlp::launch_adam(params, grads, m, v, step, lr, beta1, beta2, epsilon, weights, biases,
+                   static_cast<cudaStream_t>(stream));
+  return cuda_status(cudaGetLastError());
+}
+
+int msb_cell_features(msb_context* context, const msb_cell_arrays* cells, uint16_t* features) {
+  if (context == nullptr || cells == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  auto& c = *context;
+  return guarded(context, [&] {
+    if (cells->count > 0 && features == nullptr) throw std::invalid_argument("null features");
+    msb_cell_arrays copy = *cells;
+    load_cells(c, copy, true);
+    compute_features(c, c.state.view());
+    if (c.n > 0) {
+      check(cudaMemcpyAsync(features, c.features.p, std::size_t(c.n) * mlp::kInput * 2, cudaMemcpyDeviceToDevice,
+                            c.stream),
+            "copy features");
+    }
+    sync(c);
+  });
+}
+
+int msb_set_warm_start_network(msb_context* context, const uint16_t* weights, const float* biases,
+                               const float* scale) {
+  if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  auto& c = *context;
+  return guarded(context, [&] {
+    c.has_network = false;
+    if (weights == nullptr) return;
+    if (biases == nullptr || scale == nullptr) throw std::invalid_argument("null network biases or scale");
+    for (int k = 0; k < 3; ++k) {
+      if (!std::isfinite(scale[k]) || !(scale[k] > 0.0f)) throw std::invalid_argument("network scale must be positive");
+      c.net_scale[k] = scale[k];
+    }
+    c.net_weights.ensure(mlp::kWeights);
+    c.net_biases.ensure(mlp::kBiases);
+    check(cudaMemcpyAsync(c.net_weights.p, weights, mlp::kWeights * 2ull, cudaMemcpyDefault, c.stream), "weights");
+    check(cudaMemcpyAsync(c.net_biases.p, biases, mlp::kBiases * 4ull, cudaMemcpyDefault, c.stream), "biases");
+    sync(c);
+    c.has_network = true;
+  });
 }
 
 int msb_set_motion_guess(msb_context* context, const float* guess, uint64_t cell_count, float dt) {

@@ -160,6 +160,7 @@ def test_motion_guess_serves_one_step_and_checks_its_size(fresh):
 def test_warm_start_flags_are_checked(fresh):
     lib = abi.load_library()
     assert lib.msb_set_warm_start(fresh._handle, 3) == abi.OK
-    assert lib.msb_set_warm_start(fresh._handle, 4) == abi.ERR_INVALID_ARGUMENT
+    assert lib.msb_set_warm_start(fresh._handle, 7) == abi.OK
+    assert lib.msb_set_warm_start(fresh._handle, 8) == abi.ERR_INVALID_ARGUMENT
     assert lib.msb_set_warm_start(None, 0) == abi.ERR_INVALID_ARGUMENT
     assert lib.msb_set_warm_start(fresh._handle, 0) == abi.OK
