@@ -57,6 +57,9 @@ def parse():
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--no-learned", action="store_true")
+    p.add_argument("--train-cells", type=int, default=200_000)
+    p.add_argument("--train-steps", type=int, default=1500)
     return p.parse_args()
 
 
@@ -234,6 +237,49 @@ def reference_arm(args):
     }))
 
 
+def learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrier, dist):
+    """The learned warm start: a network trained on the GPU on trajectories
+    of the plain stepper on a separate colony of the same distribution
+    (args.train_cells capsules), then the same K steps as the plain
+    measurement from the same state with the network's guess (flag 4) and
+    with the guess plus the previous step's forces (flags 4 | 1)."""
+    import torch
+
+    from microsimulator_b200 import learned, workloads
+
+    device = f"cuda:{local}"
+    t0 = time.perf_counter()
+    train_world = workloads.jammed(n=args.train_cells, seed=args.seed + 1000 + rank)
+    for k in range(25):  # the random start's overlaps relax
+        device_step(train_world, 5000 + k)
+    net, report = learned.train_warm_start(
+        backend, train_world, dynamics(), DT, lambda w, k: divide(w, 6000 + k, args.seed + rank),
+        collect_steps=4, train_steps=args.train_steps, seed=args.seed, device=device)
+    training_s = time.perf_counter() - t0
+    net.install(backend)
+    out = {"training": {"cells": args.train_cells, "samples": report.samples,
+                        "validation_samples": report.validation_samples, "adam_steps": report.steps,
+                        "validation_mse": report.validation_loss,
+                        "zero_guess_mse": report.validation_variance,
+                        "seconds_with_data": training_s}}
+    for name, mode in (("learned", 4), ("learned_carry", 5), ("carry", 1)):
+        world = snapshot.copy()
+        device_step(world.copy(), args.warmup - 1, mode)  # one untimed step in this mode
+        backend.set_warm_start(0)  # forget its forces: the timed steps start as the plain ones do
+        barrier()
+        total_ms, cell_steps, iterations, phases = timed(world, mode)
+        barrier()
+        if dist is not None:
+            t = torch.tensor([total_ms], device=device, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            total_ms = float(t.item())
+        world_size = dist.get_world_size() if dist is not None else 1
+        out[name] = {"value": cell_steps * world_size / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
+                     "bb_iterations_per_step": iterations / args.steps, "phase_ms_per_step": phases}
+    backend.set_warm_start(0)
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -265,7 +311,8 @@ def main():
     world = workloads.jammed(n=args.cells, seed=args.seed + rank)
     dyn = dynamics()
 
-    def device_step(step):
+    def device_step(world, step, mode=0):
+        backend.set_warm_start(mode)
         divide(world, step, args.seed + rank)
         cells = DeviceCells(world, device=f"cuda:{local}")
         torch.cuda.synchronize()
@@ -278,23 +325,27 @@ def main():
         world.next_id = int(world.ids.max()) + 1
         return start.elapsed_time(end), report
 
-    for step in range(args.warmup):
-        device_step(step)
-    snapshot = world.copy()
-    barrier()
-    launches0 = backend.launch_count()
-    total_ms = 0.0
-    cell_steps = 0
-    iterations = 0
-    phases = {name: 0.0 for name in backend.PHASES}
-    with Clocks(local) as clocks:
+    def timed(world, mode):
+        """K steps from `world`; device time, cell-steps, iterations and
+        phases."""
+        total_ms, cell_steps, iterations = 0.0, 0, 0
+        phases = {name: 0.0 for name in backend.PHASES}
         for k in range(args.steps):
-            ms, report = device_step(args.warmup + k)
+            ms, report = device_step(world, args.warmup + k, mode)
             total_ms += ms
             cell_steps += len(world)  # the cells of the step (divisions run before it)
             iterations += report.iterations
             for name, value in backend.last_step_phases().items():
                 phases[name] += value / args.steps
+        return total_ms, cell_steps, iterations, phases
+
+    for step in range(args.warmup):
+        device_step(world, step)
+    snapshot = world.copy()
+    barrier()
+    launches0 = backend.launch_count()
+    with Clocks(local) as clocks:
+        total_ms, cell_steps, iterations, phases = timed(world, 0)
     barrier()
     launches = backend.launch_count() - launches0
     prof = backend.profile_iterations(20)
@@ -302,7 +353,7 @@ def main():
     # e2e: the same steps from the same state through the host-buffer call.
     e2e = None
     if not args.no_e2e:
-        world = snapshot
+        world = snapshot.copy()
         e2e_s = 0.0
         e2e_cells = 0
         h2d = d2h = 0
@@ -325,6 +376,10 @@ def main():
             e2e_total = float(t.item())
         e2e = {"value": e2e_cells * world_size / e2e_total, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
+
+    learned = None
+    if not args.no_learned:
+        learned = learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrier, dist)
 
     total = total_ms
     if dist is not None:
@@ -362,8 +417,9 @@ def main():
             "dtype": "f32",
             "data": "synthetic",
             "config": config(args, world_size),
-            "path": "plain",
+            "path": "plain (zero-start multipliers: the reference's semantics)",
             "bb_iterations_per_step": iterations / args.steps,
+            "learned": learned,
             "phase_ms_per_step": phases,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",
