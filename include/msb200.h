@@ -456,6 +456,51 @@ int msb_mlp_adam(float* params, const float* grads, float* m, float* v, uint32_t
 int msb_set_warm_start_network(msb_context* context, const uint16_t* weights, const float* biases,
                                const float* scale);
 
+/* ---- Batches of independent colonies (no counterpart in the reference) --
+ *
+ * One contact-dynamics step of many independent colonies at once, as a
+ * parameter sweep runs them.  The cells of all colonies are passed colony
+ * after colony in one msb_cell_arrays (ids unique across the batch); each
+ * colony has its own drag and contact stiffness (replacing those of
+ * `dynamics`, whose other parameters all colonies share).  Colonies never
+ * touch one another, wherever their cells lie: the contact search's grid
+ * gives each colony its own range of boxes.
+ *
+ * Each colony's contacts and rows are those it would have alone.  Each
+ * colony's solves run their own Barzilai-Borwein iteration (own step length,
+ * residual, tolerance and iteration count) to its own tolerance, all colonies
+ * in one persistent launch of thread-block clusters.  The substep plan is the
+ * batch's: a colony whose substep fails the rotation or overlap checks makes
+ * the whole batch halve, and growth bounds are the batch's largest.
+ * Constraints (walls) are not taken.  Warm-start flags other than carry are
+ * rejected.
+ *
+ * The first call on a context tunes the launch shape of the batched solve
+ * (CTAs per cluster, threads per CTA) and the box scale of the contact search
+ * by timing each candidate on that call's system; msb_tune_batch asks for a
+ * new tuning at the next call and msb_batch_tuning reads the choice. */
+typedef struct msb_colony_parameters {
+  float drag;
+  float contact_stiffness;
+} msb_colony_parameters;
+
+typedef struct msb_colony_report {
+  uint64_t iterations; /* BB iterations of this colony's solves over the step */
+  float max_overlap;   /* deepest overlap at the accepted geometry */
+  uint32_t rows;       /* rows of the colony's last solved system */
+  uint32_t cells;
+  uint32_t reserved;
+} msb_colony_report;
+
+int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* cells, const uint32_t* colony_cells,
+                                       uint32_t colony_count, const msb_colony_parameters* colony_parameters,
+                                       float dt, const msb_contact_dynamics_parameters* dynamics,
+                                       const msb_contact_parameters* contacts, msb_contact_dynamics_report* report,
+                                       msb_colony_report* colony_reports, msb_contact_dynamics_outputs* outputs,
+                                       int device_pointers);
+int msb_tune_batch(msb_context* context);
+int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, float* box_scale);
+
 /* Device time of the last msb_advance_contact_dynamics(_device) call by
  * phase, measured with CUDA events on the context's stream, in
  * milliseconds: [0] upload, validation and id order; [1] contact searches;

@@ -218,7 +218,14 @@ class ContactDynamicsOutputs(ctypes.Structure):
     ]
 
 
+class ColonyParameters(ctypes.Structure):
+    _fields_ = [("drag", c_float), ("contact_stiffness", c_float)]
+
+
 # numpy views of the record types, for bulk conversion.
+COLONY_REPORT_DTYPE = np.dtype([("iterations", "<u8"), ("max_overlap", "<f4"), ("rows", "<u4"), ("cells", "<u4"),
+                                ("reserved", "<u4")])
+
 CELL_CONTACT_DTYPE = np.dtype(
     [
         ("first_id", "<u8"),
@@ -374,6 +381,10 @@ SIGNATURES = {
     "msb_launch_count": (c_uint64, [c_void_p]),
     "msb_last_step_phases": (c_int, [c_void_p, c_void_p, c_uint32]),
     "msb_set_warm_start": (c_int, [c_void_p, c_uint32]),
+    "msb_advance_contact_dynamics_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_float, c_void_p,
+                                                   c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
+    "msb_tune_batch": (c_int, [c_void_p]),
+    "msb_batch_tuning": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "msb_cell_features": (c_int, [c_void_p, c_void_p, c_void_p]),
     "msb_mlp_activation_bytes": (c_uint64, [c_uint64]),
     "msb_mlp_backward_scratch_bytes": (c_uint64, [c_uint64]),

@@ -251,6 +251,42 @@ class B200Backend:
             ctypes.byref(cp), ctypes.byref(wp), ctypes.byref(report), ctypes.byref(outputs)))
         return ContactDynamicsResult(ContactDynamicsReport.from_native(report), velocities, loads, increments)
 
+    def advance_contact_dynamics_batch(self, cells, colony_cells, drag, stiffness, dt: float,
+                                       dynamics: ContactDynamicsParameters | None = None,
+                                       contacts: ContactParameters | None = None, outputs=None):
+        """One step of a batch of independent colonies laid out colony after
+        colony in ``cells`` (a WorldState, updated in place, or DeviceCells),
+        each with its own drag and contact stiffness.  Returns the batch's
+        report and one ``abi.COLONY_REPORT_DTYPE`` record per colony."""
+        dynamics = dynamics or ContactDynamicsParameters()
+        contacts = contacts or ContactParameters()
+        counts = np.ascontiguousarray(colony_cells, dtype=np.uint32)
+        k = counts.shape[0]
+        params = (abi.ColonyParameters * k)()
+        for i, (d, s) in enumerate(zip(np.asarray(drag, np.float32), np.asarray(stiffness, np.float32))):
+            params[i] = abi.ColonyParameters(float(d), float(s))
+        reports = np.zeros(k, dtype=abi.COLONY_REPORT_DTYPE)
+        report = abi.ContactDynamicsReport()
+        dyn, cp = dynamics.native(), contacts.native()
+        device = isinstance(cells, DeviceCells)
+        arrays = cells.arrays()
+        native_outputs = outputs.native() if outputs is not None else None
+        self._check(self._lib.msb_advance_contact_dynamics_batch(
+            self._handle, ctypes.byref(arrays), c_void_p(abi.ptr(counts)), k, ctypes.byref(params), c_float(dt),
+            ctypes.byref(dyn), ctypes.byref(cp), ctypes.byref(report), c_void_p(abi.ptr(reports)),
+            ctypes.byref(native_outputs) if native_outputs is not None else None, 1 if device else 0))
+        return ContactDynamicsReport.from_native(report), reports
+
+    def tune_batch(self) -> None:
+        """Ask for a new tuning of the batched launch at the next batch call."""
+        self._check(self._lib.msb_tune_batch(self._handle))
+
+    def batch_tuning(self) -> dict:
+        cluster, threads, scale = ctypes.c_uint32(0), ctypes.c_uint32(0), c_float(0)
+        self._check(self._lib.msb_batch_tuning(self._handle, ctypes.byref(cluster), ctypes.byref(threads),
+                                               ctypes.byref(scale)))
+        return {"cluster": cluster.value, "threads": threads.value, "box_scale": scale.value}
+
     def advance_contact_dynamics_device(self, cells: "DeviceCells", constraints, dt: float,
                                         dynamics: ContactDynamicsParameters | None = None,
                                         contacts: ContactParameters | None = None,

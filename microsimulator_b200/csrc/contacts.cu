@@ -77,7 +77,8 @@ __global__ void cell_bounds_kernel(GeometryView g, float margin, double* __restr
 }
 
 __global__ void grid_setup_kernel(const double* __restrict__ partials, std::uint32_t partial_count,
-                                  std::uint32_t cells, std::uint64_t bucket_capacity, GridParams* grid) {
+                                  std::uint32_t cells, std::uint64_t bucket_capacity, GridParams* grid,
+                                  double box_scale, std::uint32_t colonies) {
   // Block reduction of the per-block partials (minima, maxima, finite flag).
   __shared__ double shared[10][kThreads / 32];
   double v[10];
@@ -112,7 +113,7 @@ __global__ void grid_setup_kernel(const double* __restrict__ partials, std::uint
   for (int a = 0; a < 3; ++a) {
     // Boxes 0.1% wider than the widest padded capsule keep rounding from
     // putting overlapping capsules two boxes apart.
-    const double box_width = smax(v[6 + a] * 1.001, DBL_MIN);
+    const double box_width = smax(v[6 + a] * 1.001 * box_scale, DBL_MIN);
     const double extent = floor((v[3 + a] - v[a]) / box_width) + 1.0;
     out.low[a] = v[a];
     out.inv_width[a] = 1.0 / box_width;
@@ -125,6 +126,15 @@ __global__ void grid_setup_kernel(const double* __restrict__ partials, std::uint
     }
   }
   if (!(boxes <= limit)) dense = false;
+  if (colonies > 0) {
+    // A batch: each colony gets its own range of z boxes, two boxes apart
+    // from the next colony's, in a hashed table.
+    const double extent = floor((v[5] - v[2]) * out.inv_width[2]) + 1.0;
+    const double stride = extent + 2.0;
+    if (!(stride * double(colonies) < 9.0e15)) out.status = 1u;
+    out.colony_stride = std::uint32_t(smin(stride, 4.0e9));
+    dense = false;
+  }
   if (dense) {
     out.hashed = 0;
     out.buckets = std::uint32_t(boxes);
@@ -137,18 +147,22 @@ __global__ void grid_setup_kernel(const double* __restrict__ partials, std::uint
       const double extent = floor((v[3 + a] - v[a]) * out.inv_width[a]) + 1.0;
       out.dims[a] = extent < 9.0e15 ? std::uint64_t(extent) : 9000000000000000ull;
     }
+    if (colonies > 0) out.dims[2] = std::uint64_t(out.colony_stride) * colonies;
   }
   if (out.buckets + 1ull > bucket_capacity) out.status = 2u;
   *grid = out;
 }
 
-__device__ __forceinline__ void box_of(const double* b, const GridParams& grid, std::int64_t at[3]) {
+__device__ __forceinline__ void box_of(const double* b, const GridParams& grid, std::int64_t at[3],
+                                       std::uint32_t colony) {
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
     const double centre = 0.5 * (b[a] + b[3 + a]);
     const double position = smax(0.0, (centre - grid.low[a]) * grid.inv_width[a]);
-    const double top = double(grid.dims[a] - 1);
+    const bool stacked = a == 2 && grid.colony_stride > 0;
+    const double top = stacked ? double(grid.colony_stride - 3) : double(grid.dims[a] - 1);
     at[a] = std::int64_t(smin(top, floor(position)));
+    if (stacked) at[a] += std::int64_t(colony) * std::int64_t(grid.colony_stride);
   }
 }
 
@@ -171,7 +185,7 @@ __global__ void bin_cells_kernel(GeometryView g, const double* __restrict__ boun
   if (grid.status != 0) return;
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.count; i += gridDim.x * blockDim.x) {
     std::int64_t at[3];
-    box_of(bounds + 6 * std::uint64_t(i), grid, at);
+    box_of(bounds + 6 * std::uint64_t(i), grid, at, g.colony != nullptr ? g.colony[i] : 0u);
     const std::uint32_t b = bucket_of(grid, at[0], at[1], at[2]);
     cell_bucket[i] = b;
     if (grid.hashed) {
@@ -231,7 +245,7 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
 #pragma unroll
     for (int q = 0; q < 6; ++q) box[q] = bounds[6 * std::uint64_t(a) + q];
     std::int64_t at[3];
-    box_of(box, grid, at);
+    box_of(box, grid, at, g.colony != nullptr ? g.colony[a] : 0u);
     std::int64_t first[3], last[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
@@ -890,8 +904,10 @@ void launch_cell_bounds(GeometryView g, float margin, double* bounds, double* pa
 }
 
 void launch_grid_setup(const double* partials, std::uint32_t partial_count, std::uint32_t cells,
-                       std::uint64_t bucket_capacity, GridParams* grid, cudaStream_t stream) {
-  grid_setup_kernel<<<1, kThreads, 0, stream>>>(partials, partial_count, cells, bucket_capacity, grid);
+                       std::uint64_t bucket_capacity, GridParams* grid, cudaStream_t stream, float box_scale,
+                       std::uint32_t colonies) {
+  grid_setup_kernel<<<1, kThreads, 0, stream>>>(partials, partial_count, cells, bucket_capacity, grid,
+                                                double(box_scale), colonies);
   count_launch();
 }
 

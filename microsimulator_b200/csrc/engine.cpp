@@ -25,6 +25,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/msb200.h"
+#include "batch.h"
 #include "kernels.h"
 #include "solve.h"
 #include "step.h"
@@ -168,6 +169,7 @@ constexpr std::uint32_t kRotationProbeIterations = 128;
 constexpr float kSolveToleranceFraction = 0.25f;
 constexpr float kLoadResolutionFraction = 0.1f;
 constexpr std::uint32_t kEasyRefinements = 2;
+constexpr std::uint32_t kMaxColonies = 1u << 20;
 // Warm-start flags (msb_set_warm_start).
 constexpr std::uint32_t kWarmCarry = 1;       // the previous step's final forces
 constexpr std::uint32_t kWarmGuess = 2;    // forces that a motion guess asks of each body
@@ -352,6 +354,26 @@ struct msb_context {
   msb::DBuf<float4> inc_a, inc_b, resp_a, resp_b, accepted_a, accepted_b;
   msb::DBuf<float> slack;
 
+  // A batch of independent colonies (msb_advance_contact_dynamics_batch);
+  // colonies == 0 for a single system.
+  std::uint32_t colonies = 0;
+  std::vector<std::uint32_t> host_colony_offsets;
+  msb::DBuf<std::uint32_t> colony_offsets, colony_of_slot, colony_order, colony_overlap, colony_rows,
+      colony_row_counts, colony_row_offsets, batch_next;
+  msb::DBuf<float> colony_drag, colony_stiffness, colony_tolerance, colony_solve_tolerance, colony_slack,
+      batch_saved;
+  msb::DBuf<msb::ColonyState> colony_state;
+  std::vector<msb::ColonyState> host_colony_state;
+  std::vector<std::uint64_t> colony_iterations;
+  std::vector<float> colony_max_overlap;
+  std::vector<std::uint32_t> colony_rows_at_accept;
+  msb::BatchShape batch_shape{4, 256};
+  int batch_clusters = 0;
+  bool batch_tuned = false;
+  float box_scale = 1.0f;        // the contact search's box scale for the current call
+  float batch_box_scale = 1.0f;  // the autotuner's choice for batches
+  bool tune_search = true;
+
   // solve
   int last_blocks = 0;
   msb::SolveDesc* desc = nullptr;
@@ -432,6 +454,7 @@ void read_scalars(Ctx& c) {
     const auto code = c.host_scalars[kStatus];
     if (code == kStatusGeometry) throw std::invalid_argument("cell geometry is invalid (non-finite, negative or unnormalized)");
     if (code == kStatusIndex) throw std::invalid_argument("cell identifiers must be non-zero and unique");
+
     throw DeviceCheckError("a device-side check failed (code " + std::to_string(code) + ")");
   }
 }
@@ -450,9 +473,16 @@ std::uint32_t read_u32(Ctx& c, const std::uint32_t* device_ptr) {
   return v;
 }
 
-GeometryView view_of(Ctx& c, Geometry& g) { return {g.pos_len.p, g.dir_rad.p, c.ids.p, c.n}; }
+GeometryView view_of(Ctx& c, Geometry& g) {
+  return {g.pos_len.p, g.dir_rad.p, c.ids.p, c.n, c.colonies > 0 ? c.colony_of_slot.p : nullptr};
+}
 
 // ---- cells ---------------------------------------------------------------
+
+Colonies colonies_of(Ctx& c) {
+  if (c.colonies == 0) return {};
+  return {c.colony_of_slot.p, c.colony_drag.p, c.colony_stiffness.p, c.colony_overlap.p, c.colony_slack.p};
+}
 
 void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
   if (cells.count >= 0xFFFFFFF0ull) throw std::overflow_error("cell count exceeds the slot index space");
@@ -553,7 +583,7 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   c.grid.ensure(1);
   launch_cell_bounds(g, prm.margin, c.bounds.p, c.bound_partials.p, c.stream);
   const std::uint64_t capacity = grid_bucket_capacity(n);
-  launch_grid_setup(c.bound_partials.p, partials, n, capacity, c.grid.p, c.stream);
+  launch_grid_setup(c.bound_partials.p, partials, n, capacity, c.grid.p, c.stream, c.box_scale, c.colonies);
   c.cell_bucket.ensure(n);
   c.coords.ensure(3ull * n);
   c.bucket_counts.ensure(capacity);
@@ -699,8 +729,11 @@ void build_row_keys(Ctx& c, RowStore& store) {
 
 // Runs the solve graph on c.rows (multipliers in place).  Requires the
 // incidence of c.rows and the bodies.
+SolveOutcome solve_batch(Ctx& c, float dt, const msb_growth_load_response& growth, std::uint32_t max_iterations);
+
 SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, float tolerance,
                    std::uint32_t max_iterations) {
+  if (c.colonies > 0) return solve_batch(c, dt, growth, max_iterations);
   const std::uint32_t rows = c.rows.count;
   c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
   c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
@@ -721,6 +754,128 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
   c.solve_log.push_back({rows, d.iterations, d.status, d.residual});
   if (d.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
   return {d.status, d.iterations, d.residual};
+}
+
+// The batched solve over c.rows: rows grouped by colony, one persistent
+// launch of clusters (see batch.h), per-colony state read back.  The outcome
+// is the batch's worst status and its largest iteration count; each
+// colony's iterations accumulate in c.colony_iterations.
+msb::BatchDesc batch_desc(Ctx& c, float dt, const msb_growth_load_response& growth, std::uint32_t max_iterations) {
+  msb::BatchDesc d{};
+  d.rows = c.rows.arrays();
+  d.bodies = {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
+  d.incidence = {c.inc_offsets.p, c.inc_a.p, c.inc_b.p};
+  d.response = {c.resp_a.p, c.resp_b.p};
+  d.multipliers = c.rows.multipliers.p;
+  d.gaps = c.rows.gaps.p;
+  d.colony_rows = c.colony_rows.p;
+  d.row_offsets = c.colony_row_offsets.p;
+  d.cell_offsets = c.colony_offsets.p;
+  d.order = c.colony_order.p;
+  d.tolerance = c.colony_solve_tolerance.p;
+  d.state = c.colony_state.p;
+  d.next = c.batch_next.p;
+  d.colonies = c.colonies;
+  d.dt = dt;
+  d.law = growth.law;
+  d.sensitivity = growth.sensitivity;
+  d.free_load = growth.free_load;
+  d.stall_load = growth.stall_load;
+  d.max_iterations = max_iterations;
+  d.has_drift = c.has_drift ? 1u : 0u;
+  return d;
+}
+
+void run_batch(Ctx& c, const msb::BatchDesc& d, msb::BatchShape shape, int clusters) {
+  check(cudaMemsetAsync(c.batch_next.p, 0, 4, c.stream), "memset");
+  check(cudaError_t(launch_batch_solve(d, shape, clusters, c.stream)), "batched solve launch");
+}
+
+// The project's autotuner for the batched solve: times each launch shape
+// (CTAs per cluster x threads per CTA) on the system at hand, from the same
+// start multipliers, and keeps the fastest.
+void tune_batch(Ctx& c, const msb::BatchDesc& d) {
+  const std::uint32_t rows = c.rows.count;
+  c.batch_saved.ensure(std::max<std::uint32_t>(rows, 1));
+  check(cudaMemcpyAsync(c.batch_saved.p, c.rows.multipliers.p, rows * 4ull, cudaMemcpyDeviceToDevice, c.stream),
+        "save multipliers");
+  cudaEvent_t start, stop;
+  check(cudaEventCreate(&start), "event");
+  check(cudaEventCreate(&stop), "event");
+  float best = -1.0f;
+  for (const int threads : {256, 512}) {
+    for (const int cluster : {1, 2, 4, 8}) {
+      const msb::BatchShape shape{cluster, threads};
+      const int resident = batch_resident_clusters(shape);
+      if (resident <= 0) continue;
+      const int clusters = std::min<int>(resident, int(c.colonies));
+      check(cudaMemcpyAsync(c.rows.multipliers.p, c.batch_saved.p, rows * 4ull, cudaMemcpyDeviceToDevice, c.stream),
+            "restore multipliers");
+      check(cudaEventRecord(start, c.stream), "event");
+      run_batch(c, d, shape, clusters);
+      check(cudaEventRecord(stop, c.stream), "event");
+      check(cudaEventSynchronize(stop), "event");
+      float ms = 0.0f;
+      check(cudaEventElapsedTime(&ms, start, stop), "event");
+      if (best < 0.0f || ms < best) {
+        best = ms;
+        c.batch_shape = shape;
+        c.batch_clusters = clusters;
+      }
+    }
+  }
+  cudaEventDestroy(start);
+  cudaEventDestroy(stop);
+  if (best < 0.0f) throw std::runtime_error("no launch shape of the batched solve fits the device");
+  check(cudaMemcpyAsync(c.rows.multipliers.p, c.batch_saved.p, rows * 4ull, cudaMemcpyDeviceToDevice, c.stream),
+        "restore multipliers");
+  c.batch_tuned = true;
+}
+
+SolveOutcome solve_batch(Ctx& c, float dt, const msb_growth_load_response& growth, std::uint32_t max_iterations) {
+  const std::uint32_t rows = c.rows.count;
+  const std::uint32_t k = c.colonies;
+  c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
+  c.colony_rows.ensure(std::max<std::uint32_t>(rows, 1));
+  c.sort_keys.ensure(std::max<std::uint32_t>(rows, 1));
+  c.colony_row_counts.ensure(k + 1ull);
+  c.colony_row_offsets.ensure(k + 1ull);
+  c.temp.ensure(sort_temp_words(rows + 1ull) + scan_temp_words(k + 1ull) + 64);
+  check(cudaMemsetAsync(c.colony_row_counts.p, 0, (k + 1ull) * 4, c.stream), "memset");
+  launch_colony_row_keys(c.rows.slots.p, rows, c.colony_of_slot.p, c.sort_keys.p, c.colony_rows.p,
+                         c.colony_row_counts.p, c.stream);
+  exclusive_scan(c.colony_row_counts.p, c.colony_row_offsets.p, k + 1ull, c.temp.p, c.stream);
+  if (rows > 1) radix_sort_pairs(c.sort_keys.p, c.colony_rows.p, rows, std::max(1, int(std::bit_width(k))), c.temp.p,
+                                 c.stream);
+  const msb::BatchDesc d = batch_desc(c, dt, growth, max_iterations);
+  if (!c.batch_tuned) tune_batch(c, d);
+  run_batch(c, d, c.batch_shape, c.batch_clusters);
+  c.host_colony_state.resize(k);
+  check(cudaMemcpyAsync(c.host_colony_state.data(), c.colony_state.p, k * sizeof(msb::ColonyState),
+                        cudaMemcpyDeviceToHost, c.stream),
+        "read colony states");
+  sync(c);
+  SolveOutcome out{};
+  out.status = MSB_SOLVE_CONVERGED;
+  std::uint32_t worst = 0;
+  float residual = 0.0f;
+  for (std::uint32_t i = 0; i < k; ++i) {
+    const auto& st = c.host_colony_state[i];
+    if (st.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
+    c.colony_iterations[i] += st.iterations;
+    out.iterations = std::max(out.iterations, st.iterations);
+    residual = std::max(residual, st.residual);
+    if (st.status == MSB_SOLVE_BREAKDOWN) {
+      worst = 2;
+    } else if (st.status != MSB_SOLVE_CONVERGED && worst < 1) {
+      worst = 1;
+    }
+  }
+  out.status = worst == 2 ? MSB_SOLVE_BREAKDOWN : (worst == 1 ? MSB_SOLVE_ITERATION_LIMIT : MSB_SOLVE_CONVERGED);
+  out.residual = residual;
+  c.solve_log.push_back({rows, out.iterations, out.status, residual});
+  return out;
 }
 
 // ---- the substep and the step -------------------------------------------
@@ -751,8 +906,9 @@ Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_const
   c.flag_offsets.ensure(o.candidates + 1ull);
   reset_scalars(c);
   check(cudaMemsetAsync(c.flags.p + o.candidates, 0, 4, c.stream), "memset");
+  if (c.colonies > 0) check(cudaMemsetAsync(c.colony_overlap.p, 0, c.colonies * 4ull, c.stream), "memset");
   launch_recheck(c.found.p, o.candidates, c.rows.keyed(), c.slack.p, p.wall_stiffness, p.contact_stiffness,
-                 c.flags.p, c.scalars.p + kOverlapBits, c.stream);
+                 c.flags.p, c.scalars.p + kOverlapBits, c.stream, colonies_of(c));
   c.temp.ensure(scan_temp_words(o.candidates + 1ull) + 64);
   exclusive_scan(c.flags.p, c.flag_offsets.p, o.candidates + 1ull, c.temp.p, c.stream);
   check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 4, c.flag_offsets.p + o.candidates, 4,
@@ -773,7 +929,7 @@ void append_overlap_rows(Ctx& c, const Overlaps& o, const ResponseArrays& respon
   const std::uint32_t base_row = c.rows.count;
   c.rows.grow(std::size_t(base_row) + o.overlapping, c.stream);
   launch_make_rows(c.flagged.p, o.overlapping, c.trial.view(), build, &response, c.rows.arrays(), base_row,
-                   c.rows.partner.p, c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
+                   c.rows.partner.p, c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream, colonies_of(c));
   c.rows.count = base_row + o.overlapping;
   build_row_keys(c, c.rows);
 }
@@ -872,7 +1028,7 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   c.drift_b.ensure(n);
   mark(c, kPhaseRows);
   launch_make_bodies(n, c.state.view(), c.growth.p, c.fixed.p, c.initial.view(), p.drag,
-                     {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream);
+                     {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream, colonies_of(c));
   mark(c, kPhaseSearch);
   const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches);
   mark(c, kPhaseRows);
@@ -880,12 +1036,17 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   c.rows.ensure(std::max<std::uint32_t>(found, 1));
   reset_scalars(c);
   const RowBuild build{p.wall_stiffness, p.contact_stiffness, p.max_overlap_recovery, dt};
+  if (c.colonies > 0) check(cudaMemsetAsync(c.colony_overlap.p, 0, c.colonies * 4ull, c.stream), "memset");
   launch_make_rows(c.touches.p, found, c.base.view(), build, nullptr, c.rows.arrays(), 0, c.rows.partner.p,
-                   c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream);
+                   c.rows.multipliers.p, c.scalars.p + kOverlapBits, c.stream, colonies_of(c));
   c.rows.count = found;
   const float tolerance = effective_overlap_tolerance(p);
   c.slack.ensure(1);
   launch_slack(c.scalars.p + kOverlapBits, tolerance, p.max_overlap_recovery, c.slack.p, c.stream);
+  if (c.colonies > 0) {
+    launch_colony_slack(c.colonies, c.colony_overlap.p, c.colony_tolerance.p, p.max_overlap_recovery,
+                        c.colony_slack.p, c.stream);
+  }
   build_row_keys(c, c.rows);
   const KeyedLists memory = c.memory.keyed();
   const MemoryCells cells{c.memory_first_ids.p, c.memory_partner_ids.p, c.ids.p, c.memory_cells};
@@ -936,6 +1097,19 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
 
     const Overlaps found_overlaps = flag_overlaps(c, cp, wp, p);
     if (found_overlaps.overlapping == 0) {
+      if (c.colonies > 0) {
+        // Each colony's deepest overlap at the accepted geometry and its rows.
+        std::vector<std::uint32_t> bits(c.colonies);
+        c.colony_rows_at_accept.resize(c.colonies);
+        check(cudaMemcpyAsync(bits.data(), c.colony_overlap.p, c.colonies * 4ull, cudaMemcpyDeviceToHost, c.stream),
+              "read overlaps");
+        check(cudaMemcpyAsync(c.colony_rows_at_accept.data(), c.colony_row_counts.p, c.colonies * 4ull,
+                              cudaMemcpyDeviceToHost, c.stream),
+              "read rows");
+        sync(c);
+        c.colony_max_overlap.resize(c.colonies);
+        for (std::uint32_t i = 0; i < c.colonies; ++i) c.colony_max_overlap[i] = bits_to_float(bits[i]);
+      }
       attempt.accepted = true;
       attempt.refinements = refinement;
       attempt.rows = c.rows.count;
@@ -1564,6 +1738,161 @@ int msb_advance_contact_dynamics(msb_context* context, msb_cell_arrays* cells, c
                                  msb_contact_dynamics_report* report, msb_contact_dynamics_outputs* outputs) {
   return advance_entry(context, cells, constraints, constraint_count, dt, dynamics, contacts, constraint_parameters,
                        report, outputs, false);
+}
+
+int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* cells, const uint32_t* colony_cells,
+                                       uint32_t colony_count, const msb_colony_parameters* colony_parameters,
+                                       float dt, const msb_contact_dynamics_parameters* dynamics,
+                                       const msb_contact_parameters* contacts, msb_contact_dynamics_report* report,
+                                       msb_colony_report* colony_reports, msb_contact_dynamics_outputs* outputs,
+                                       int device_pointers) {
+  if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  return guarded(context, [&] {
+    if (cells == nullptr || dynamics == nullptr || report == nullptr || colony_cells == nullptr ||
+        colony_parameters == nullptr || colony_reports == nullptr) {
+      throw std::invalid_argument("null argument");
+    }
+    if (colony_count == 0 || colony_count > kMaxColonies) {
+      throw std::invalid_argument("a batch holds 1 to " + std::to_string(kMaxColonies) + " colonies");
+    }
+    if (!std::isfinite(dt) || dt < 0.0f) throw std::invalid_argument("time step must be finite and non-negative");
+    const msb_contact_parameters cp = contacts != nullptr ? *contacts : msb_contact_parameters{0.01f, 0.1f, 1.0e-6f};
+    const msb_constraint_contact_parameters wp{0.0f, 1.0e-6f};
+    validate_dynamics(*dynamics);
+    validate_contact_parameters(cp);
+    auto& c = *context;
+    if ((c.warm_start_mode & ~kWarmCarry) != 0) {
+      throw std::invalid_argument("a batch takes no motion guess or warm-start network");
+    }
+    std::vector<std::uint32_t> offsets(colony_count + 1, 0);
+    std::vector<float> drag(colony_count), stiffness(colony_count), tolerance(colony_count), solve_tol(colony_count);
+    for (std::uint32_t i = 0; i < colony_count; ++i) {
+      offsets[i + 1] = offsets[i] + colony_cells[i];
+      if (offsets[i + 1] < offsets[i]) throw std::overflow_error("too many cells");
+      const auto& q = colony_parameters[i];
+      if (!std::isfinite(q.drag) || !(q.drag > 0.0f) || !std::isfinite(q.contact_stiffness) ||
+          !(q.contact_stiffness > 0.0f)) {
+        throw std::invalid_argument("colony drag and contact stiffness must be positive and finite");
+      }
+      msb_contact_dynamics_parameters own = *dynamics;
+      own.drag = q.drag;
+      own.contact_stiffness = q.contact_stiffness;
+      validate_dynamics(own);
+      drag[i] = q.drag;
+      stiffness[i] = q.contact_stiffness;
+      tolerance[i] = effective_overlap_tolerance(own);
+      solve_tol[i] = kSolveToleranceFraction * tolerance[i];
+    }
+    if (offsets.back() != cells->count) throw std::invalid_argument("colony cell counts must sum to the cell count");
+    // Largest colonies first in the solve's work queue.
+    std::vector<std::uint32_t> order(colony_count);
+    for (std::uint32_t i = 0; i < colony_count; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](std::uint32_t a, std::uint32_t b) { return colony_cells[a] > colony_cells[b]; });
+
+    struct Reset {
+      Ctx& c;
+      ~Reset() {
+        c.colonies = 0;
+        c.box_scale = 1.0f;
+      }
+    } reset{c};
+    c.box_scale = c.batch_box_scale;
+    c.phase_marks.clear();
+    c.solve_log.clear();
+    mark(c, kPhaseLoad);
+    load_cells(c, *cells, device_pointers != 0);
+    c.constraint_count = 0;
+    c.colonies = colony_count;
+    c.host_colony_offsets = offsets;
+    c.colony_offsets.ensure(colony_count + 1ull);
+    c.colony_order.ensure(colony_count);
+    c.colony_drag.ensure(colony_count);
+    c.colony_stiffness.ensure(colony_count);
+    c.colony_tolerance.ensure(colony_count);
+    c.colony_solve_tolerance.ensure(colony_count);
+    c.colony_overlap.ensure(colony_count);
+    c.colony_slack.ensure(colony_count);
+    c.colony_state.ensure(colony_count);
+    c.batch_next.ensure(1);
+    c.colony_of_slot.ensure(std::max<std::uint32_t>(c.n, 1));
+    const auto up = [&](void* dst, const void* src, std::size_t bytes) {
+      check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, c.stream), "copy colonies");
+    };
+    up(c.colony_offsets.p, offsets.data(), offsets.size() * 4);
+    up(c.colony_order.p, order.data(), order.size() * 4);
+    up(c.colony_drag.p, drag.data(), drag.size() * 4);
+    up(c.colony_stiffness.p, stiffness.data(), stiffness.size() * 4);
+    up(c.colony_tolerance.p, tolerance.data(), tolerance.size() * 4);
+    up(c.colony_solve_tolerance.p, solve_tol.data(), solve_tol.size() * 4);
+    launch_colony_of_slot(colony_count, c.colony_offsets.p, c.n, c.colony_of_slot.p, c.stream);
+    c.has_memory = c.has_memory && (c.warm_start_mode & kWarmCarry) != 0;
+    c.colony_iterations.assign(colony_count, 0);
+    c.colony_max_overlap.assign(colony_count, 0.0f);
+    c.colony_rows_at_accept.assign(colony_count, 0);
+    if (c.tune_search && c.n > 1) {
+      // The autotuner's search leg: the box scale with the fastest contact
+      // search on this batch (every scale finds the same contacts).
+      cudaEvent_t start, stop;
+      check(cudaEventCreate(&start), "event");
+      check(cudaEventCreate(&stop), "event");
+      float best = -1.0f, chosen = 1.0f;
+      for (const float scale : {1.0f, 1.5f, 2.0f, 3.0f}) {
+        c.box_scale = scale;
+        find_touches(c, c.state, cp, wp, dynamics->candidate_margin, c.touches);  // warm
+        check(cudaEventRecord(start, c.stream), "event");
+        find_touches(c, c.state, cp, wp, dynamics->candidate_margin, c.touches);
+        check(cudaEventRecord(stop, c.stream), "event");
+        check(cudaEventSynchronize(stop), "event");
+        float ms = 0.0f;
+        check(cudaEventElapsedTime(&ms, start, stop), "event");
+        if (best < 0.0f || ms < best) {
+          best = ms;
+          chosen = scale;
+        }
+      }
+      cudaEventDestroy(start);
+      cudaEventDestroy(stop);
+      c.box_scale = chosen;
+      c.batch_box_scale = chosen;
+      c.tune_search = false;
+    }
+    StepOutcome outcome;
+    try {
+      outcome = advance(c, dt, *dynamics, cp, wp);
+    } catch (...) {
+      c.has_memory = false;
+      throw;
+    }
+    mark(c, kPhaseOutput);
+    write_back(c, *cells, device_pointers != 0);
+    write_outputs(c, outputs, device_pointers != 0);
+    mark(c, kPhaseEnd);
+    sync(c);
+    collect_phases(c);
+    *report = outcome.report;
+    for (std::uint32_t i = 0; i < colony_count; ++i) {
+      colony_reports[i] = {c.colony_iterations[i], c.colony_max_overlap[i],
+                           i < c.colony_rows_at_accept.size() ? c.colony_rows_at_accept[i] : 0u, colony_cells[i]};
+    }
+  });
+}
+
+int msb_tune_batch(msb_context* context) {
+  if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  context->batch_tuned = false;
+  context->tune_search = true;
+  return MSB_OK;
+}
+
+int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, float* box_scale) {
+  if (context == nullptr || cluster == nullptr || threads == nullptr || box_scale == nullptr) {
+    return MSB_ERR_INVALID_ARGUMENT;
+  }
+  *cluster = std::uint32_t(context->batch_shape.cluster);
+  *threads = std::uint32_t(context->batch_shape.threads);
+  *box_scale = context->batch_box_scale;
+  return MSB_OK;
 }
 
 int msb_advance_contact_dynamics_device(msb_context* context, msb_cell_arrays* cells,

@@ -39,6 +39,10 @@ struct GeometryView {
   const float4* dir_rad;
   const std::uint64_t* ids;
   std::uint32_t count;
+  // For a batch of independent colonies, the colony of each slot: the grid
+  // gives every colony its own range of z boxes, so that no two colonies'
+  // cells are ever candidates of one another.  Null for one system.
+  const std::uint32_t* colony = nullptr;
 };
 
 // One contact of a cell with a cell (s2 valid) or with a constraint (s2 =
@@ -80,7 +84,7 @@ struct GridParams {
   std::uint32_t hashed;   // 0: dense boxes (x * dy + y) * dz + z; 1: hashed table
   std::uint32_t buckets;  // buckets in use
   std::uint32_t status;
-  std::uint32_t pad;
+  std::uint32_t colony_stride;  // z boxes per colony of a batch (0: one system)
 };
 
 // ---- primitives.cu
@@ -106,8 +110,11 @@ std::uint32_t bound_partials(std::uint32_t cells);
 // Padded FP64 boxes (6 doubles per cell) and the grid over them.
 void launch_cell_bounds(GeometryView g, float margin, double* bounds, double* partials,
                         cudaStream_t stream);
+// Boxes are box_scale (>= 1) times the widest padded capsule: any scale finds
+// the same pairs, and the best one depends on the density.
 void launch_grid_setup(const double* partials, std::uint32_t partial_count, std::uint32_t cells,
-                       std::uint64_t bucket_capacity, GridParams* grid, cudaStream_t stream);
+                       std::uint64_t bucket_capacity, GridParams* grid, cudaStream_t stream, float box_scale = 1.0f,
+                       std::uint32_t colonies = 0);
 void launch_bin_cells(GeometryView g, const double* bounds, const GridParams* grid,
                       std::uint32_t* cell_bucket, std::int64_t* cell_coords, std::uint32_t* bucket_counts,
                       cudaStream_t stream);

@@ -56,8 +56,9 @@ __global__ void unpack_cells_kernel(std::uint32_t n, GeometryBuffers in, float* 
 
 __global__ void make_bodies_kernel(std::uint32_t n, GeometryBuffers state, const float* __restrict__ growth,
                                    const std::uint8_t* __restrict__ fixed, GeometryBuffers rate_lengths,
-                                   float drag, BodyArrays bodies) {
+                                   float colony_drag, BodyArrays bodies, Colonies colonies) {
   for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    const float drag = colonies.of_slot != nullptr ? colonies.drag[colonies.of_slot[s]] : colony_drag;
     const float4 pl = state.pos_len[s];
     const float4 dr = state.dir_rad[s];
     const float rate = growth[s] * rate_lengths.pos_len[s].w;
@@ -102,11 +103,13 @@ __device__ __forceinline__ float wrench_dot(float4 ja, float4 jb, float4 va, flo
 __global__ void make_rows_kernel(const Touch* __restrict__ touches, std::uint32_t count, GeometryBuffers geometry,
                                  RowBuild prm, ResponseArrays response, int correct, RowArrays rows,
                                  std::uint32_t row_base, std::uint64_t* __restrict__ key_partner,
-                                 float* __restrict__ multipliers, std::uint32_t* overlap_bits) {
+                                 float* __restrict__ multipliers, std::uint32_t* overlap_bits, Colonies colonies) {
   for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
     const Touch t = touches[k];
     const bool wall = t.s2 == kInvalidSlot;
-    const float compliance = 1.0f / (wall ? prm.wall_stiffness : prm.contact_stiffness);
+    const std::uint32_t colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
+    const float stiffness = colonies.of_slot != nullptr ? colonies.stiffness[colony] : prm.contact_stiffness;
+    const float compliance = 1.0f / (wall ? prm.wall_stiffness : stiffness);
     float offset = smax(t.sep, -prm.recovery);
     const float c = t.sep < -prm.recovery ? compliance * prm.recovery / -t.sep : compliance;
     const F3 n{t.normal[0], t.normal[1], t.normal[2]};
@@ -143,6 +146,7 @@ __global__ void make_rows_kernel(const Touch* __restrict__ touches, std::uint32_
     key_partner[i] = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
     multipliers[i] = 0.0f;
     atomic_max_nonnegative(overlap_bits, -t.sep);
+    if (colonies.overlap_bits != nullptr) atomic_max_nonnegative(colonies.overlap_bits + colony, -t.sep);
   }
 }
 
@@ -334,11 +338,14 @@ __global__ void restore_kernel(std::uint32_t n, GeometryBuffers src, GeometryBuf
 
 __global__ void recheck_kernel(const Touch* __restrict__ touches, std::uint32_t count, KeyedLists current,
                                const float* slack_ptr, float wall_stiffness, float contact_stiffness,
-                               std::uint32_t* __restrict__ flags, std::uint32_t* overlap_bits) {
-  const float slack = *slack_ptr;
+                               std::uint32_t* __restrict__ flags, std::uint32_t* overlap_bits, Colonies colonies) {
   for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
     const Touch t = touches[k];
     atomic_max_nonnegative(overlap_bits, -t.sep);
+    const std::uint32_t colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
+    if (colonies.overlap_bits != nullptr) atomic_max_nonnegative(colonies.overlap_bits + colony, -t.sep);
+    const float slack = colonies.slack != nullptr ? colonies.slack[colony] : *slack_ptr;
+    if (colonies.stiffness != nullptr) contact_stiffness = colonies.stiffness[colony];
     const bool wall = t.s2 == kInvalidSlot;
     const std::uint64_t key = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
     float force = 0.0f;
@@ -364,6 +371,31 @@ __global__ void slack_kernel(const std::uint32_t* overlap_bits, float tolerance,
   if (threadIdx.x == 0) {
     const float starting = __uint_as_float(*overlap_bits);
     *slack = tolerance + smax(0.0f, starting - recovery);
+  }
+}
+
+__global__ void colony_slack_kernel(std::uint32_t colonies, const std::uint32_t* overlap_bits,
+                                    const float* tolerance, float recovery, float* slack) {
+  for (std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < colonies; c += gridDim.x * blockDim.x) {
+    const float starting = __uint_as_float(overlap_bits[c]);
+    slack[c] = tolerance[c] + smax(0.0f, starting - recovery);
+  }
+}
+
+__global__ void colony_of_slot_kernel(std::uint32_t colonies, const std::uint32_t* __restrict__ offsets,
+                                      std::uint32_t n, std::uint32_t* __restrict__ of_slot) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+    // The last colony whose first slot is at or before s.
+    std::uint32_t lo = 0, hi = colonies;
+    while (hi - lo > 1) {
+      const std::uint32_t mid = (lo + hi) / 2;
+      if (offsets[mid] <= s) {
+        lo = mid;
+      } else {
+        hi = mid;
+      }
+    }
+    of_slot[s] = lo;
   }
 }
 
@@ -458,22 +490,23 @@ void launch_unpack_cells(std::uint32_t n, GeometryBuffers in, float* px, float* 
 }
 
 void launch_make_bodies(std::uint32_t n, GeometryBuffers state, const float* growth_rates, const std::uint8_t* fixed,
-                        GeometryBuffers rate_lengths, float drag, BodyArrays bodies, cudaStream_t stream) {
+                        GeometryBuffers rate_lengths, float drag, BodyArrays bodies, cudaStream_t stream,
+                        Colonies colonies) {
   if (n == 0) return;
   make_bodies_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, state, growth_rates, fixed, rate_lengths,
-                                                                      drag, bodies);
+                                                                      drag, bodies, colonies);
   count_launch();
 }
 
 void launch_make_rows(const Touch* touches, std::uint32_t count, GeometryBuffers geometry, RowBuild prm,
                       const ResponseArrays* response, RowArrays rows, std::uint32_t row_base,
                       std::uint64_t* key_partner, float* multipliers, std::uint32_t* overlap_bits,
-                      cudaStream_t stream) {
+                      cudaStream_t stream, Colonies colonies) {
   if (count == 0) return;
   const ResponseArrays none{nullptr, nullptr};
   make_rows_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(
       touches, count, geometry, prm, response != nullptr ? *response : none, response != nullptr ? 1 : 0, rows,
-      row_base, key_partner, multipliers, overlap_bits);
+      row_base, key_partner, multipliers, overlap_bits, colonies);
   count_launch();
 }
 
@@ -537,10 +570,10 @@ void launch_restore(std::uint32_t n, GeometryBuffers src, GeometryBuffers dst, s
 
 void launch_recheck(const Touch* touches, std::uint32_t count, KeyedLists current, const float* slack,
                     float wall_stiffness, float contact_stiffness, std::uint32_t* flags, std::uint32_t* overlap_bits,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, Colonies colonies) {
   if (count == 0) return;
   recheck_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(touches, count, current, slack, wall_stiffness,
-                                                                      contact_stiffness, flags, overlap_bits);
+                                                                      contact_stiffness, flags, overlap_bits, colonies);
   count_launch();
 }
 
@@ -554,6 +587,21 @@ void launch_gather_flagged(const Touch* touches, std::uint32_t count, const std:
 void launch_slack(const std::uint32_t* overlap_bits, float tolerance, float recovery, float* slack,
                   cudaStream_t stream) {
   slack_kernel<<<1, 32, 0, stream>>>(overlap_bits, tolerance, recovery, slack);
+  count_launch();
+}
+
+void launch_colony_slack(std::uint32_t colonies, const std::uint32_t* overlap_bits, const float* tolerance,
+                         float recovery, float* slack, cudaStream_t stream) {
+  if (colonies == 0) return;
+  colony_slack_kernel<<<grid_for(colonies, kThreads), kThreads, 0, stream>>>(colonies, overlap_bits, tolerance,
+                                                                             recovery, slack);
+  count_launch();
+}
+
+void launch_colony_of_slot(std::uint32_t colonies, const std::uint32_t* offsets, std::uint32_t n,
+                           std::uint32_t* of_slot, cudaStream_t stream) {
+  if (n == 0 || colonies == 0) return;
+  colony_of_slot_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(colonies, offsets, n, of_slot);
   count_launch();
 }
 

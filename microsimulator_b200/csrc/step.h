@@ -17,6 +17,18 @@ struct GeometryBuffers {
 
 constexpr std::uint64_t kWallTag = 1ull << 63;
 
+// A batch of independent colonies stepped together: the colony of each cell
+// slot and each colony's drag and contact stiffness, and each colony's
+// deepest overlap (bits of a non-negative float) and overlap slack.  All
+// null for a single system, whose scalar parameters apply.
+struct Colonies {
+  const std::uint32_t* of_slot;
+  const float* drag;
+  const float* stiffness;
+  std::uint32_t* overlap_bits;
+  const float* slack;
+};
+
 // Packs SoA cell arrays (device pointers) into float4 geometry, checking
 // what WorldState::validate checks.  status: kStatusGeometry on bad input.
 void launch_pack_cells(std::uint32_t n, const float* px, const float* py, const float* pz, const float* dx,
@@ -28,7 +40,8 @@ void launch_unpack_cells(std::uint32_t n, GeometryBuffers in, float* px, float* 
 // make_bodies (contact_dynamics.cpp:257-284).
 // Elongation rates use the lengths of `rate_lengths` (the step's initial geometry).
 void launch_make_bodies(std::uint32_t n, GeometryBuffers state, const float* growth_rates, const std::uint8_t* fixed,
-                        GeometryBuffers rate_lengths, float drag, BodyArrays bodies, cudaStream_t stream);
+                        GeometryBuffers rate_lengths, float drag, BodyArrays bodies, cudaStream_t stream,
+                        Colonies colonies = {});
 
 // make_row over `count` touches into rows [row_base, row_base + count), with
 // their keys; the deepest overlap goes to *overlap_bits.  With `response`,
@@ -42,7 +55,7 @@ struct RowBuild {
 void launch_make_rows(const Touch* touches, std::uint32_t count, GeometryBuffers geometry, RowBuild prm,
                       const ResponseArrays* response, RowArrays rows, std::uint32_t row_base,
                       std::uint64_t* key_partner, float* multipliers, std::uint32_t* overlap_bits,
-                      cudaStream_t stream);
+                      cudaStream_t stream, Colonies colonies = {});
 
 // Initial multipliers from the previous substep's forces (ForceMemory).
 struct KeyedLists {
@@ -96,12 +109,18 @@ void launch_restore(std::uint32_t n, GeometryBuffers src, GeometryBuffers dst, s
 // touches deeper than the slack plus what their own force presses in.
 void launch_recheck(const Touch* touches, std::uint32_t count, KeyedLists current, const float* slack,
                     float wall_stiffness, float contact_stiffness, std::uint32_t* flags, std::uint32_t* overlap_bits,
-                    cudaStream_t stream);
+                    cudaStream_t stream, Colonies colonies = {});
 void launch_gather_flagged(const Touch* touches, std::uint32_t count, const std::uint32_t* flags,
                            const std::uint32_t* offsets, Touch* out, cudaStream_t stream);
 // The substep slack: tolerance + max(0, deepest - recovery).
 void launch_slack(const std::uint32_t* overlap_bits, float tolerance, float recovery, float* slack,
                   cudaStream_t stream);
+// The slack of each colony of a batch from its deepest overlap and tolerance.
+void launch_colony_slack(std::uint32_t colonies, const std::uint32_t* overlap_bits, const float* tolerance,
+                         float recovery, float* slack, cudaStream_t stream);
+// colony_of_slot[s] for cells laid out colony after colony (offsets: colonies + 1).
+void launch_colony_of_slot(std::uint32_t colonies, const std::uint32_t* offsets, std::uint32_t n,
+                           std::uint32_t* of_slot, cudaStream_t stream);
 // Largest growth per step, in radii (contact_dynamics.cpp:700-706).
 void launch_growth_bound(std::uint32_t n, GeometryBuffers state, const float* growth_rates, float dt,
                          std::uint32_t* bits, cudaStream_t stream);

@@ -55,6 +55,16 @@ def jammed(n: int = 1_000_000, area_fraction: float = 0.85, seed: int = 42, grow
     return _planar(rng, n, (0.0, 0.0), (side, side), lengths, growth_rate)
 
 
+def sweep_colony(n: int, seed: int = 42, area_fraction: float = 0.7, growth_rate: float = 0.5) -> WorldState:
+    """One colony of a parameter sweep: N capsules with the shapes of the
+    trap workload (radius 0.5 um, lengths U[2, 4] um) packed at the area
+    fraction in an open square domain."""
+    rng = np.random.default_rng(seed)
+    lengths = rng.uniform(2.0, 4.0, n)
+    side = math.sqrt(n * mean_capsule_area(float(np.mean(lengths))) / area_fraction)
+    return _planar(rng, n, (0.0, 0.0), (side, side), lengths, growth_rate)
+
+
 def jammed_side(n: int, area_fraction: float = 0.85) -> float:
     return math.sqrt(n * mean_capsule_area(3.0 * math.exp(0.02)) / area_fraction)
 

@@ -1,0 +1,160 @@
+"""Batched colonies through msb_advance_contact_dynamics_batch: each colony
+of a batch steps as it would alone (same rows; positions within the solve's
+tolerance-level spread), with its own drag, stiffness and convergence, and
+colonies that overlap in space never touch."""
+
+import numpy as np
+import pytest
+
+from microsimulator_b200 import sweep, workloads
+from microsimulator_b200.backend import B200Backend, DeviceCells
+from microsimulator_b200.types import ContactDynamicsParameters
+
+pytestmark = pytest.mark.gpu
+
+TOLERANCE = 5e-4
+DT = 0.02
+SIZES = [300, 1500, 700, 50, 1100, 400]
+DRAG = [1.0, 0.6, 1.7, 1.2, 0.9, 2.0]
+STIFFNESS = [1.0e4, 0.5e4, 2.0e4, 1.3e4, 0.8e4, 1.0e4]
+
+_SETTLED = {}
+
+
+def params(k):
+    return ContactDynamicsParameters(overlap_tolerance=TOLERANCE, drag=DRAG[k], contact_stiffness=STIFFNESS[k])
+
+
+def settled_worlds():
+    """Each colony settled alone for 20 steps with its own parameters."""
+    if "worlds" not in _SETTLED:
+        b = B200Backend(0)
+        worlds = []
+        try:
+            for k, n in enumerate(SIZES):
+                w = workloads.sweep_colony(n, seed=100 + k)
+                for step in range(20):
+                    plan = workloads.plan_divisions(w, 0.02, seed=step * 31 + k)
+                    w.divide_many(plan.parents, 0.5, plan.rotations)
+                    b.advance_contact_dynamics(w, None, DT, params(k))
+                    w.next_id = int(w.ids.max()) + 1
+                worlds.append(w)
+        finally:
+            b.close()
+        _SETTLED["worlds"] = worlds
+    return [w.copy() for w in _SETTLED["worlds"]]
+
+
+def test_each_colony_steps_as_it_would_alone(backend):
+    worlds = settled_worlds()
+    alone = [w.copy() for w in worlds]
+    reports_alone = [backend.advance_contact_dynamics(w, None, DT, params(k)).report for k, w in enumerate(alone)]
+    batch = sweep.ColonyBatch(worlds, DRAG, STIFFNESS)
+    b = B200Backend(0)
+    try:
+        report, colonies = batch.step(b, DT, ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+        tuning = b.batch_tuning()
+    finally:
+        b.close()
+    assert tuning["cluster"] in (1, 2, 4, 8) and tuning["threads"] in (256, 512)
+    assert tuning["box_scale"] >= 1.0
+    assert np.array_equal(colonies["cells"], np.array(SIZES_after(worlds), dtype=np.uint32))
+    same_plan = report.substeps == 1 and all(r.substeps == 1 for r in reports_alone)
+    for k, (w, a, r) in enumerate(zip(batch.worlds, alone, reports_alone)):
+        assert np.array_equal(w.ids, a.ids)
+        spread = np.max(np.abs(w.geometry()[:, :3] - a.geometry()[:, :3]))
+        if same_plan and r.refinements == report.refinements:
+            # The same rows as alone, and a position spread at the solve's tolerance level.
+            assert colonies["rows"][k] == r.max_rows, (k, colonies["rows"][k], r.max_rows)
+            assert spread < 4 * TOLERANCE, (k, spread)
+        else:
+            assert spread < 0.05, (k, spread)
+        assert np.all(np.isfinite(w.geometry()))
+        assert colonies["iterations"][k] > 0 or r.iterations == 0
+
+
+def SIZES_after(worlds):
+    return [len(w) for w in worlds]
+
+
+def test_colony_parameters_reach_their_colony(backend):
+    """Two copies of one colony with different drag move differently; the
+    same colony twice with the same parameters moves identically."""
+    w = settled_worlds()[1]
+    batch = sweep.ColonyBatch([w.copy(), w.copy(), w.copy()], [1.0, 1.0, 2.0], [1.0e4, 1.0e4, 1.0e4])
+    b = B200Backend(0)
+    try:
+        batch.step(b, DT, ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+    finally:
+        b.close()
+    a, same, slow = (x.geometry() for x in batch.worlds)
+    assert np.array_equal(a, same)
+    assert not np.array_equal(a, slow)
+
+
+def test_colonies_in_the_same_place_never_touch(backend):
+    """Colonies are laid out in the same region of space; a batch of a
+    colony and a shifted copy steps each as alone."""
+    w = settled_worlds()[2]
+    shifted = w.copy()
+    shifted.position_x = shifted.position_x + np.float32(1.3)
+    alone = [w.copy(), shifted.copy()]
+    reports = [backend.advance_contact_dynamics(a, None, DT, params(0)).report for a in alone]
+    batch = sweep.ColonyBatch([w.copy(), shifted.copy()], [DRAG[0]] * 2, [STIFFNESS[0]] * 2)
+    b = B200Backend(0)
+    try:
+        report, colonies = batch.step(b, DT, ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+    finally:
+        b.close()
+    for k in range(2):
+        if report.substeps == reports[k].substeps == 1 and report.refinements == reports[k].refinements:
+            assert colonies["rows"][k] == reports[k].max_rows
+        spread = np.max(np.abs(batch.worlds[k].geometry()[:, :3] - alone[k].geometry()[:, :3]))
+        assert spread < 0.05
+
+
+def test_device_batch_equals_host_batch(backend):
+    worlds = settled_worlds()[:3]
+    batch = sweep.ColonyBatch(worlds, DRAG[:3], STIFFNESS[:3])
+    host = batch.concatenated()
+    device = DeviceCells(host.copy())
+    b = B200Backend(0)
+    try:
+        rh, ch = b.advance_contact_dynamics_batch(host, batch.counts(), batch.drag, batch.stiffness, DT,
+                                                  ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+        # The second call reuses the first call's tuning.
+        fresh = batch.concatenated()
+        device = DeviceCells(fresh)
+        rd, cd = b.advance_contact_dynamics_batch(device, batch.counts(), batch.drag, batch.stiffness, DT,
+                                                  ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+    finally:
+        b.close()
+    out = batch.concatenated()
+    device.download(out)
+    assert rh == rd
+    assert np.array_equal(ch, cd)
+    assert np.array_equal(host.geometry(), out.geometry())
+
+
+def test_batch_rejects_what_it_cannot_step(backend):
+    w = settled_worlds()[3]
+    batch = sweep.ColonyBatch([w], [1.0], [1.0e4])
+    cells = batch.concatenated()
+    p = ContactDynamicsParameters(overlap_tolerance=TOLERANCE)
+    with pytest.raises(ValueError):
+        backend.advance_contact_dynamics_batch(cells, [len(cells) - 1], [1.0], [1.0e4], DT, p)
+    with pytest.raises(ValueError):
+        backend.advance_contact_dynamics_batch(cells, [len(cells)], [0.0], [1.0e4], DT, p)
+    bad = cells.copy()
+    bad.position_x = bad.position_x.copy()
+    bad.position_x[0] = np.nan
+    before = bad.copy()
+    with pytest.raises(ValueError):
+        backend.advance_contact_dynamics_batch(bad, [len(cells)], [1.0], [1.0e4], DT, p)
+    assert np.array_equal(before.geometry(), bad.geometry(), equal_nan=True)
+    backend.set_warm_start(backend.WARM_START_GUESS)
+    try:
+        with pytest.raises(ValueError):
+            backend.advance_contact_dynamics_batch(cells, [len(cells)], [1.0], [1.0e4], DT, p)
+    finally:
+        backend.set_warm_start(0)
