@@ -58,6 +58,8 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true")
+    p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--sweep-colonies", type=int, default=256)
     p.add_argument("--train-cells", type=int, default=200_000)
     p.add_argument("--train-steps", type=int, default=1500)
     return p.parse_args()
@@ -280,6 +282,79 @@ def learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrie
     return out
 
 
+def sweep_arm(args, backend, local, rank, dist):
+    """The parameter sweep: args.sweep_colonies independent colonies
+    (log-uniform sizes in [500, 50,000], per-colony stiffness and drag
+    factors in [0.5, 2], trap-workload capsule shapes at area fraction 0.7),
+    stepped together through the batch C-ABI with cells resident in HBM;
+    beside it the same colonies stepped one call each from the same state."""
+    import torch
+
+    from microsimulator_b200 import sweep
+    from microsimulator_b200.backend import DeviceCells
+
+    device = f"cuda:{local}"
+    batch = sweep.sweep_batch(count=args.sweep_colonies, seed=args.seed + rank)
+    dyn = dynamics()
+
+    def step(k):
+        batch.divide(DIVISION_FRACTION, seed=args.seed * 1000 + k)
+        cat = batch.concatenated()
+        cells = DeviceCells(cat, device=device)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        report, colonies = backend.advance_contact_dynamics_batch(cells, batch.counts(), batch.drag, batch.stiffness,
+                                                                  DT, dyn)
+        end.record()
+        torch.cuda.synchronize()
+        cells.download(cat)
+        sweep.split_into(cat, batch.worlds)
+        for w in batch.worlds:
+            w.next_id = int(w.ids.max()) + 1
+        return start.elapsed_time(end), report, colonies, len(cat)
+
+    for k in range(max(args.warmup, 3)):
+        step(k)
+    before = [w.copy() for w in batch.worlds]
+    total_ms, cell_steps, iterations, unconverged = 0.0, 0, 0, 0
+    for k in range(args.steps):
+        ms, report, colonies, n = step(100 + k)
+        total_ms += ms
+        cell_steps += n
+        iterations += int(colonies["iterations"].sum())
+    tuning = backend.batch_tuning()
+    # The same colonies one call each, one step, from the state before the timed steps.
+    one = sweep.ColonyBatch([w.copy() for w in before], batch.drag, batch.stiffness)
+    one.divide(DIVISION_FRACTION, seed=args.seed * 1000 + 100)
+    sequential_ms, sequential_cells = 0.0, 0
+    from microsimulator_b200.types import ContactDynamicsParameters
+
+    for w, d, st in zip(one.worlds, one.drag, one.stiffness):
+        p = ContactDynamicsParameters(overlap_tolerance=TOLERANCE, drag=float(d), contact_stiffness=float(st))
+        cells = DeviceCells(w, device=device)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        backend.advance_contact_dynamics_device(cells, None, DT, p)
+        torch.cuda.synchronize()
+        sequential_ms += (time.perf_counter() - t0) * 1e3
+        sequential_cells += len(w)
+    sizes = batch.counts()
+    return {
+        "workload": f"{len(batch)} colonies, {int(sizes.min())}..{int(sizes.max())} capsules (log-uniform 500..50000), "
+                    "drag and stiffness factors U[0.5, 2], lengths U[2, 4] um, area fraction 0.7, growth 0.5, "
+                    "2% divisions/step, tol 5e-4 um",
+        "cells": int(sizes.sum()),
+        "value": cell_steps / (total_ms * 1e-3),
+        "unit": "cell-steps/s",
+        "ms_per_step": total_ms / args.steps,
+        "bb_iterations_per_step_summed_over_colonies": iterations / args.steps,
+        "tuning": tuning,
+        "one_call_per_colony": {"value": sequential_cells / (sequential_ms * 1e-3), "unit": "cell-steps/s",
+                                "ms_per_step": sequential_ms, "timing": "host wall clock around each device call"},
+    }
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -377,6 +452,9 @@ def main():
         e2e = {"value": e2e_cells * world_size / e2e_total, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
+    sweep_line = None
+    if not args.no_sweep:
+        sweep_line = sweep_arm(args, backend, local, rank, dist)
     learned = None
     if not args.no_learned:
         learned = learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrier, dist)
@@ -420,6 +498,7 @@ def main():
             "path": "plain (zero-start multipliers: the reference's semantics)",
             "bb_iterations_per_step": iterations / args.steps,
             "learned": learned,
+            "sweep": sweep_line,
             "phase_ms_per_step": phases,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",
