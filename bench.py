@@ -161,9 +161,11 @@ def measured_peak():
 
 
 def ncu_traffic():
-    """DRAM bytes per BB iteration per row and per body from the committed ncu
-    summary (profiles/bb_iteration_traffic.json), scaled to a launch by the
-    system's size; None without one."""
+    """DRAM bytes of one BB iteration as a multiple of its algorithmic bytes,
+    from the committed ncu capture (profiles/bb_iteration_traffic.json, a
+    500,000-capsule system); None without one.  The bench scales it to its own
+    launch by the algorithmic bytes, which grow with rows and bodies as the
+    traffic does."""
     path = ROOT / "profiles" / "bb_iteration_traffic.json"
     if not path.exists():
         return None
@@ -474,7 +476,7 @@ def main():
     traffic = ncu_traffic()
     traffic_bytes = None
     if traffic is not None:
-        traffic_bytes = rows * traffic["bytes_per_row"] + bodies * traffic["bytes_per_body"]
+        traffic_bytes = algorithmic * traffic["ratio_to_algorithmic"]
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
