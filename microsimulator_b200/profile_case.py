@@ -17,12 +17,21 @@ colony (``features_kernel``, ``forward_kernel``), timed with CUDA events:
 the first call's autotuner launches the kernel once per launch shape first):
 
   python -m microsimulator_b200.profile_case --case batch --colonies 64
+
+--case guess: the upper bound of any motion-guess warm start.  Each step of a
+jammed colony runs plain, then again from the same state with the plain
+step's own displacement as the guess (warm-start flag 2) and with carried
+forces (flag 1); prints the iterations of each solve of each:
+
+  python -m microsimulator_b200.profile_case --case guess --cells 1000000 --warm 3 --steps 3
 """
 
 from __future__ import annotations
 
 import argparse
 import json
+
+import numpy as np
 
 
 def mlp_case(args) -> None:
@@ -72,9 +81,68 @@ def batch_case(args) -> None:
     backend.close()
 
 
+def guess_case(args) -> None:
+    import torch
+
+    from . import workloads
+    from .backend import B200Backend, DeviceCells
+    from .types import ContactDynamicsParameters
+
+    backend = B200Backend(0)
+    dyn = ContactDynamicsParameters(overlap_tolerance=5e-4)
+    world = workloads.jammed(n=args.cells, seed=args.seed)
+
+    def run(w, mode, guess=None):
+        backend.set_warm_start(mode)
+        if guess is not None:
+            backend.set_motion_guess(guess, 0.02)
+        cells = DeviceCells(w)
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        report = backend.advance_contact_dynamics_device(cells, None, 0.02, dyn)
+        end.record()
+        torch.cuda.synchronize()
+        cells.download(w)
+        w.next_id = int(w.ids.max()) + 1
+        return {"ms": round(start.elapsed_time(end), 2), "iterations": report.iterations,
+                "solves": backend.last_step_solves()["iterations"].tolist()}
+
+    def divide(w, k):
+        plan = workloads.plan_divisions(w, 0.02, seed=args.seed * 100003 + k)
+        w.divide_many(plan.parents, 0.5, plan.rotations)
+
+    previous = None  # the state before step k - 1's divisions
+    for k in range(args.warm + args.steps):
+        undivided = world.copy()
+        divide(world, k)
+        before = world.copy()
+        plain = run(world, 0)
+        if k < args.warm:
+            previous = undivided
+            continue
+        exact = np.zeros((len(before), 3), np.float32)
+        exact[:, 0] = world.position_x - before.position_x
+        exact[:, 1] = world.position_y - before.position_y
+        exact[:, 2] = np.arctan2(before.direction_x * world.direction_y - before.direction_y * world.direction_x,
+                                 before.direction_x * world.direction_x + before.direction_y * world.direction_y)
+        guessed = run(before.copy(), 2, exact)
+        carried_world = previous.copy()
+        divide(carried_world, k - 1)
+        run(carried_world, 1)  # the previous step, remembered
+        divide(carried_world, k)
+        carried = run(carried_world, 1) if len(carried_world) == len(before) else None
+        backend.set_warm_start(0)
+        previous = undivided
+        print(json.dumps({"step": k, "cells": len(before), "plain": plain, "exact_guess": guessed,
+                          "carried": carried}))
+    backend.close()
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
-    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch"])
+    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess"])
+    p.add_argument("--warm", type=int, default=3)
     p.add_argument("--colonies", type=int, default=64)
     p.add_argument("--cells", type=int, default=500_000)
     p.add_argument("--steps", type=int, default=2)
@@ -86,6 +154,9 @@ def main() -> None:
         return
     if args.case == "batch":
         batch_case(args)
+        return
+    if args.case == "guess":
+        guess_case(args)
         return
 
     from . import workloads
