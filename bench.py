@@ -249,7 +249,7 @@ def learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrie
     with the guess plus the previous step's forces (flags 4 | 1)."""
     import torch
 
-    from microsimulator_b200 import learned, workloads
+    from microsimulator_b200 import learned, replicas, workloads
 
     device = f"cuda:{local}"
     t0 = time.perf_counter()
@@ -273,12 +273,9 @@ def learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrie
         barrier()
         total_ms, cell_steps, iterations, phases = timed(world, mode)
         barrier()
-        if dist is not None:
-            t = torch.tensor([total_ms], device=device, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            total_ms = float(t.item())
-        world_size = dist.get_world_size() if dist is not None else 1
-        out[name] = {"value": cell_steps * world_size / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
+        total_ms = replicas.max_over_ranks(total_ms, dist, device)
+        cells_all = replicas.sum_over_ranks(cell_steps, dist, device)
+        out[name] = {"value": cells_all / (total_ms * 1e-3), "ms_per_step": total_ms / args.steps,
                      "bb_iterations_per_step": iterations / args.steps, "phase_ms_per_step": phases}
     backend.set_warm_start(0)
     return out
@@ -295,8 +292,13 @@ def sweep_arm(args, backend, local, rank, dist):
     from microsimulator_b200 import sweep
     from microsimulator_b200.backend import DeviceCells
 
+    from microsimulator_b200 import replicas
+
     device = f"cuda:{local}"
-    batch = sweep.sweep_batch(count=args.sweep_colonies, seed=args.seed + rank)
+    full = sweep.sweep_batch(count=args.sweep_colonies, seed=args.seed)
+    world_size = dist.get_world_size() if dist is not None else 1
+    mine = replicas.shard(full.counts(), rank, world_size)  # every colony on one rank
+    batch = sweep.ColonyBatch([full.worlds[i] for i in mine], full.drag[mine], full.stiffness[mine])
     dyn = dynamics()
 
     def step(k):
@@ -320,11 +322,15 @@ def sweep_arm(args, backend, local, rank, dist):
         step(k)
     before = [w.copy() for w in batch.worlds]
     total_ms, cell_steps, iterations, unconverged = 0.0, 0, 0, 0
+    if dist is not None:
+        dist.barrier()
     for k in range(args.steps):
         ms, report, colonies, n = step(100 + k)
         total_ms += ms
         cell_steps += n
         iterations += int(colonies["iterations"].sum())
+    total_ms = replicas.max_over_ranks(total_ms, dist, device)
+    cell_steps = replicas.sum_over_ranks(cell_steps, dist, device)
     tuning = backend.batch_tuning()
     # The same colonies one call each, one step, from the state before the timed steps.
     one = sweep.ColonyBatch([w.copy() for w in before], batch.drag, batch.stiffness)
@@ -341,12 +347,15 @@ def sweep_arm(args, backend, local, rank, dist):
         torch.cuda.synchronize()
         sequential_ms += (time.perf_counter() - t0) * 1e3
         sequential_cells += len(w)
-    sizes = batch.counts()
+    sizes = full.counts()
     return {
-        "workload": f"{len(batch)} colonies, {int(sizes.min())}..{int(sizes.max())} capsules (log-uniform 500..50000), "
+        "sharding": f"{len(full)} colonies shared out over {world_size} rank(s), largest first to the least-loaded "
+                    "rank; no collective in the step",
+        "workload": f"{len(full)} colonies, {int(sizes.min())}..{int(sizes.max())} capsules (log-uniform 500..50000), "
                     "drag and stiffness factors U[0.5, 2], lengths U[2, 4] um, area fraction 0.7, growth 0.5, "
                     "2% divisions/step, tol 5e-4 um",
         "cells": int(sizes.sum()),
+        "cells_this_rank": int(batch.counts().sum()),
         "value": cell_steps / (total_ms * 1e-3),
         "unit": "cell-steps/s",
         "ms_per_step": total_ms / args.steps,
@@ -364,7 +373,7 @@ def main():
         return
     import torch
 
-    from microsimulator_b200 import workloads
+    from microsimulator_b200 import replicas, workloads
     from microsimulator_b200.backend import B200Backend, DeviceCells
 
     rank = int(os.environ.get("RANK", "0"))
@@ -446,12 +455,9 @@ def main():
             e2e_cells += n
             h2d += n * (8 + 8 * 4 + 4 + 1)
             d2h += n * (7 * 4 + 5 * 4)
-        e2e_total = e2e_s
-        if dist is not None:
-            t = torch.tensor([e2e_total], device=f"cuda:{local}", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e2e_total = float(t.item())
-        e2e = {"value": e2e_cells * world_size / e2e_total, "unit": "cell-steps/s",
+        e2e_total = replicas.max_over_ranks(e2e_s, dist, f"cuda:{local}")
+        e2e_all = replicas.sum_over_ranks(e2e_cells, dist, f"cuda:{local}")
+        e2e = {"value": e2e_all / e2e_total, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
     sweep_line = None
@@ -461,12 +467,8 @@ def main():
     if not args.no_learned:
         learned = learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrier, dist)
 
-    total = total_ms
-    if dist is not None:
-        t = torch.tensor([total_ms], device=f"cuda:{local}", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total = float(t.item())
-    value = cell_steps * world_size / (total * 1e-3)
+    total = replicas.max_over_ranks(total_ms, dist, f"cuda:{local}")
+    value = replicas.sum_over_ranks(cell_steps, dist, f"cuda:{local}") / (total * 1e-3)
 
     rows, bodies = prof["rows"], prof["bodies"]
     algorithmic = rows * 96 + bodies * 128
