@@ -221,6 +221,7 @@ __device__ __forceinline__ bool boxes_overlap(const double* l, const double* r) 
 }
 
 constexpr int kLocalPartners = 32;
+static_assert(kLocalPartners == int(kSlabPartners), "slab rows hold the locally kept partners");
 
 // One thread per cell, cells taken in bucket order so that a warp's cells
 // share their neighbour buckets in cache: the partners of higher id among
@@ -232,14 +233,20 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
                                    const float4* __restrict__ sorted_hi, const std::uint64_t* __restrict__ sorted_id,
                                    const std::int64_t* __restrict__ coords, const std::uint32_t* __restrict__ rank,
                                    std::uint32_t* __restrict__ counts, const std::uint32_t* __restrict__ offsets,
-                                   uint2* __restrict__ pairs, std::uint32_t* status) {
+                                   uint2* __restrict__ pairs, std::uint32_t* __restrict__ slab,
+                                   std::uint32_t* status) {
   const GridParams grid = *grid_ptr;
   if (grid.status != 0) return;
   const bool fill = pairs != nullptr;
+  // With a slab and no pairs, one pass counts and keeps up to kLocalPartners
+  // sorted partners per cell in its slab row; the fill pass then only runs
+  // for the cells with more.
+  const bool keep = slab != nullptr && !fill;
   for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < g.count; k += gridDim.x * blockDim.x) {
     const float4 my_lo = sorted_lo[k];
     const float4 my_hi = sorted_hi[k];
     const std::uint32_t a = __float_as_uint(my_lo.w);
+    if (fill && slab != nullptr && counts[rank[a]] <= std::uint32_t(kLocalPartners)) continue;
     const std::uint64_t id = sorted_id[k];
     double box[6];
 #pragma unroll
@@ -276,7 +283,12 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
               if (c[0] != x || c[1] != y || c[2] != z) continue;
             }
             if (!boxes_overlap(box, bounds + 6 * std::uint64_t(j))) continue;
-            if (fill) {
+            if (keep) {
+              if (found < kLocalPartners) {
+                local_id[found] = other;
+                local_slot[found] = j;
+              }
+            } else if (fill) {
               if (found < kLocalPartners) {
                 local_id[found] = other;
                 local_slot[found] = j;
@@ -288,6 +300,27 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
           }
         }
       }
+    }
+    if (keep) {
+      counts[rank[a]] = found;
+      if (found > std::uint32_t(kLocalPartners)) atomicAdd(&counts[g.count], 1u);  // cells for the fill pass
+      if (found <= kLocalPartners) {
+        for (std::uint32_t i = 1; i < found; ++i) {
+          const std::uint64_t kid = local_id[i];
+          const std::uint32_t ks = local_slot[i];
+          std::uint32_t j = i;
+          while (j > 0 && local_id[j - 1] > kid) {
+            local_id[j] = local_id[j - 1];
+            local_slot[j] = local_slot[j - 1];
+            --j;
+          }
+          local_id[j] = kid;
+          local_slot[j] = ks;
+        }
+        std::uint32_t* row = slab + std::uint64_t(rank[a]) * kLocalPartners;
+        for (std::uint32_t i = 0; i < found; ++i) row[i] = local_slot[i];
+      }
+      continue;
     }
     if (!fill) {
       counts[rank[a]] = found;
@@ -323,6 +356,22 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
       }
     }
     if (counts != nullptr && counts[rank[a]] != found) raise_status(status, kStatusCapacity);
+  }
+}
+
+// The slab rows of cells with at most kLocalPartners partners, copied into
+// their places in the pair list: thread per (cell rank, partner).
+__global__ void compact_slab_kernel(std::uint32_t n, const std::uint32_t* __restrict__ counts,
+                                    const std::uint32_t* __restrict__ offsets, const std::uint32_t* __restrict__ order,
+                                    const std::uint32_t* __restrict__ slab, uint2* __restrict__ pairs) {
+  const std::uint64_t total = std::uint64_t(n) * kLocalPartners;
+  for (std::uint64_t t = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; t < total;
+       t += std::uint64_t(gridDim.x) * blockDim.x) {
+    const std::uint32_t r = std::uint32_t(t / kLocalPartners);
+    const std::uint32_t i = std::uint32_t(t % kLocalPartners);
+    const std::uint32_t count = counts[r];
+    if (count > std::uint32_t(kLocalPartners) || i >= count) continue;
+    pairs[offsets[r] + i] = make_uint2(order[r], slab[t]);
   }
 }
 
@@ -931,10 +980,18 @@ void launch_broad_phase(GeometryView g, const double* bounds, const GridParams* 
                         const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
                         const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* rank,
                         std::uint32_t* counts, const std::uint32_t* offsets, uint2* pairs, std::uint32_t* status,
-                        cudaStream_t stream) {
+                        cudaStream_t stream, std::uint32_t* slab) {
   broad_phase_kernel<<<grid_for(g.count, 128, 16), 128, 0, stream>>>(g, bounds, grid, bucket_starts, sorted_lo,
                                                                       sorted_hi, sorted_id, cell_coords, rank, counts,
-                                                                      offsets, pairs, status);
+                                                                      offsets, pairs, slab, status);
+  count_launch();
+}
+
+void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std::uint32_t* offsets,
+                         const std::uint32_t* order, const std::uint32_t* slab, uint2* pairs, cudaStream_t stream) {
+  if (n == 0) return;
+  const std::uint64_t total = std::uint64_t(n) * kLocalPartners;
+  compact_slab_kernel<<<grid_for(total, 256), 256, 0, stream>>>(n, counts, offsets, order, slab, pairs);
   count_launch();
 }
 

@@ -322,6 +322,7 @@ struct msb_context {
   msb::DBuf<std::int64_t> coords;
   msb::DBuf<std::uint32_t> cand_counts, cand_offsets, pair_counts, pair_offsets, wall_counts, wall_offsets;
   msb::DBuf<uint2> pairs;
+  msb::DBuf<std::uint32_t> slab;  // the broad phase's kept partners, kSlabPartners per cell
   msb::DBuf<msb::Touch> touches, found, flagged;
   msb::DBuf<std::uint32_t> flags, flag_offsets;
   msb::DBuf<msb::DeviceConstraint> constraints;
@@ -601,25 +602,35 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
                        c.sorted_id.p, c.stream);
   c.cand_counts.ensure(n + 1ull);
   c.cand_offsets.ensure(n + 1ull);
+  c.slab.ensure(std::size_t(n) * kSlabPartners);
   check(cudaMemsetAsync(c.cand_counts.p + n, 0, 4, c.stream), "memset");
   reset_scalars(c);
+  // One enumeration: counts, and the partners of cells with at most
+  // kSlabPartners of them in the slab (cand_counts[n] counts the others).
   launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
-                     c.coords.p, c.rank.p, c.cand_counts.p, nullptr, nullptr, c.scalars.p + kStatus, c.stream);
+                     c.coords.p, c.rank.p, c.cand_counts.p, nullptr, nullptr, c.scalars.p + kStatus, c.stream,
+                     c.slab.p);
   exclusive_scan(c.cand_counts.p, c.cand_offsets.p, n + 1ull, c.temp.p, c.stream);
-  // grid status and the candidate total
+  // grid status, the candidate total and the cells with many partners
   GridParams grid{};
   check(cudaMemcpyAsync(&c.host_scalars[kScalarCount + 2], c.cand_offsets.p + n, 4, cudaMemcpyDeviceToHost, c.stream),
+        "read");
+  check(cudaMemcpyAsync(&c.host_scalars[kScalarCount + 3], c.cand_counts.p + n, 4, cudaMemcpyDeviceToHost, c.stream),
         "read");
   check(cudaMemcpyAsync(&grid, c.grid.p, sizeof(GridParams), cudaMemcpyDeviceToHost, c.stream), "read grid");
   read_scalars(c);
   if (grid.status == 1) throw std::invalid_argument("cell geometry is not finite");
   if (grid.status != 0) throw DeviceCheckError("grid bucket capacity exceeded");
   const std::uint32_t pair_count = c.host_scalars[kScalarCount + 2];
+  const std::uint32_t crowded = c.host_scalars[kScalarCount + 3];
   if (pair_count == 0) return 0;
   c.pairs.ensure(pair_count);
-  launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
-                     c.coords.p, c.rank.p, c.cand_counts.p, c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus,
-                     c.stream);
+  launch_compact_slab(n, c.cand_counts.p, c.cand_offsets.p, c.order.p, c.slab.p, c.pairs.p, c.stream);
+  if (crowded > 0) {
+    launch_broad_phase(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
+                       c.coords.p, c.rank.p, c.cand_counts.p, c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus,
+                       c.stream, c.slab.p);
+  }
   c.pair_counts.ensure(pair_count + 1ull);
   c.pair_offsets.ensure(pair_count + 1ull);
   c.temp.ensure(scan_temp_words(pair_count + 1ull) + scan_temp_words(capacity) + sort_temp_words(n) + 64);

@@ -129,7 +129,14 @@ void launch_broad_phase(GeometryView g, const double* bounds, const GridParams* 
                         const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
                         const std::uint64_t* sorted_id, const std::int64_t* cell_coords,
                         const std::uint32_t* rank, std::uint32_t* counts, const std::uint32_t* offsets,
-                        uint2* pairs, std::uint32_t* status, cudaStream_t stream);
+                        uint2* pairs, std::uint32_t* status, cudaStream_t stream, std::uint32_t* slab = nullptr);
+// Partners a cell's slab row holds at most; the broad phase's single-pass
+// form keeps them there (slab: cells x kSlabPartners words, by id rank).
+constexpr std::uint32_t kSlabPartners = 32;
+// Copies the slab rows of cells with at most kSlabPartners partners into
+// the pair list (counts and offsets by id rank; order: slots by id rank).
+void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std::uint32_t* offsets,
+                         const std::uint32_t* order, const std::uint32_t* slab, uint2* pairs, cudaStream_t stream);
 // Narrow phase: per candidate, the number of contacts below the margin
 // (count pass, `touches` null) or the contacts themselves at offsets[pair].
 void launch_narrow_phase(GeometryView g, const uint2* pairs, std::uint64_t pair_count,
