@@ -321,7 +321,8 @@ def sweep_arm(args, backend, local, rank, dist):
     for k in range(max(args.warmup, 3)):
         step(k)
     before = [w.copy() for w in batch.worlds]
-    total_ms, cell_steps, iterations, unconverged = 0.0, 0, 0, 0
+    total_ms, cell_steps, iterations = 0.0, 0, 0
+    phases = {name: 0.0 for name in backend.PHASES}
     if dist is not None:
         dist.barrier()
     for k in range(args.steps):
@@ -329,6 +330,8 @@ def sweep_arm(args, backend, local, rank, dist):
         total_ms += ms
         cell_steps += n
         iterations += int(colonies["iterations"].sum())
+        for name, value in backend.last_step_phases().items():
+            phases[name] += value / args.steps
     total_ms = replicas.max_over_ranks(total_ms, dist, device)
     cell_steps = replicas.sum_over_ranks(cell_steps, dist, device)
     tuning = backend.batch_tuning()
@@ -360,6 +363,7 @@ def sweep_arm(args, backend, local, rank, dist):
         "unit": "cell-steps/s",
         "ms_per_step": total_ms / args.steps,
         "bb_iterations_per_step_summed_over_colonies": iterations / args.steps,
+        "phase_ms_per_step": phases,
         "tuning": tuning,
         "one_call_per_colony": {"value": sequential_cells / (sequential_ms * 1e-3), "unit": "cell-steps/s",
                                 "ms_per_step": sequential_ms, "timing": "host wall clock around each device call"},

@@ -476,7 +476,7 @@ int msb_set_warm_start_network(msb_context* context, const uint16_t* weights, co
  * rejected.
  *
  * The first call on a context tunes the launch shape of the batched solve
- * (CTAs per cluster, threads per CTA) and the box scale of the contact search
+ * (CTAs per cluster, threads per CTA, register form) and the box scale of the contact search
  * by timing each candidate on that call's system; msb_tune_batch asks for a
  * new tuning at the next call and msb_batch_tuning reads the choice. */
 typedef struct msb_colony_parameters {
@@ -499,7 +499,11 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
                                        msb_colony_report* colony_reports, msb_contact_dynamics_outputs* outputs,
                                        int device_pointers);
 int msb_tune_batch(msb_context* context);
-int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, float* box_scale);
+/* The tuned launch: CTAs per cluster, threads per CTA, lean (1: the
+ * 64-register form of the solve kernel, one gather in flight per thread;
+ * 0: four in flight, 128 registers) and the contact search's box scale. */
+int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, uint32_t* lean,
+                     float* box_scale);
 
 /* Device time of the last msb_advance_contact_dynamics(_device) call by
  * phase, measured with CUDA events on the context's stream, in

@@ -384,7 +384,7 @@ SIGNATURES = {
     "msb_advance_contact_dynamics_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_float, c_void_p,
                                                    c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "msb_tune_batch": (c_int, [c_void_p]),
-    "msb_batch_tuning": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "msb_batch_tuning": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
     "msb_cell_features": (c_int, [c_void_p, c_void_p, c_void_p]),
     "msb_mlp_activation_bytes": (c_uint64, [c_uint64]),
     "msb_mlp_backward_scratch_bytes": (c_uint64, [c_uint64]),

@@ -282,10 +282,11 @@ class B200Backend:
         self._check(self._lib.msb_tune_batch(self._handle))
 
     def batch_tuning(self) -> dict:
-        cluster, threads, scale = ctypes.c_uint32(0), ctypes.c_uint32(0), c_float(0)
+        cluster, threads, lean, scale = ctypes.c_uint32(0), ctypes.c_uint32(0), ctypes.c_uint32(0), c_float(0)
         self._check(self._lib.msb_batch_tuning(self._handle, ctypes.byref(cluster), ctypes.byref(threads),
-                                               ctypes.byref(scale)))
-        return {"cluster": cluster.value, "threads": threads.value, "box_scale": scale.value}
+                                               ctypes.byref(lean), ctypes.byref(scale)))
+        return {"cluster": cluster.value, "threads": threads.value, "lean": bool(lean.value),
+                "box_scale": scale.value}
 
     def advance_contact_dynamics_device(self, cells: "DeviceCells", constraints, dt: float,
                                         dynamics: ContactDynamicsParameters | None = None,

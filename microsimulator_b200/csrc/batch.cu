@@ -16,10 +16,9 @@ namespace cg = cooperative_groups;
 namespace msb {
 namespace {
 
-constexpr int kBatch = 4;
-
-// Response of the colony's bodies to its (projected, with project) multipliers.
-template <int Threads>
+// Response of the colony's bodies to its (projected, with project)
+// multipliers; each thread keeps kBatch entries' gathers in flight.
+template <int kBatch>
 __device__ void colony_body_pass(const BatchDesc& d, std::uint32_t b0, std::uint32_t b1, std::uint32_t tid,
                                  std::uint32_t stride, bool project, float alpha) {
   const float* g = d.multipliers;
@@ -145,8 +144,12 @@ struct Decision {
   std::uint32_t proceed;
 };
 
-template <int Threads>
-__global__ void __launch_bounds__(Threads) batch_solve_kernel(BatchDesc d) {
+// Two forms, picked by the autotuner: Lean = false keeps 4 incidence
+// entries' gathers in flight per thread (128 registers); Lean = true one
+// (64 registers), for twice the resident warps.
+template <int Threads, bool Lean>
+__global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solve_kernel(BatchDesc d) {
+  constexpr int kBatch = Lean ? 1 : 4;
   cg::cluster_group cluster = cg::this_cluster();
   const std::uint32_t rank = cluster.block_rank();
   const std::uint32_t size = cluster.num_blocks();
@@ -187,7 +190,7 @@ __global__ void __launch_bounds__(Threads) batch_solve_kernel(BatchDesc d) {
     if ((threadIdx.x & 31) == 0 && bound > 0.0f) atomicMax(reinterpret_cast<unsigned*>(&bound_part), __float_as_uint(bound));
 
     // Mode 0: the response and gaps of the initial multipliers.
-    colony_body_pass<Threads>(d, b0, b1, tid, stride, false, 0.0f);
+    colony_body_pass<kBatch>(d, b0, b1, tid, stride, false, 0.0f);
     __threadfence();
     cluster.sync();
     Sums s = colony_row_pass(d, r0, r1, tid, stride, false, 0.0f);
@@ -229,7 +232,7 @@ __global__ void __launch_bounds__(Threads) batch_solve_kernel(BatchDesc d) {
     Decision now = *cluster.map_shared_rank(&decision, 0);
 
     while (now.proceed != 0) {
-      colony_body_pass<Threads>(d, b0, b1, tid, stride, true, now.step);
+      colony_body_pass<kBatch>(d, b0, b1, tid, stride, true, now.step);
       __threadfence();
       cluster.sync();
       s = colony_row_pass(d, r0, r1, tid, stride, true, now.step);
@@ -269,7 +272,7 @@ __global__ void __launch_bounds__(Threads) batch_solve_kernel(BatchDesc d) {
   }
 }
 
-template <int Threads>
+template <int Threads, bool Lean>
 cudaError_t launch_shape(const BatchDesc& desc, int cluster, int clusters, cudaStream_t stream) {
   cudaLaunchConfig_t config{};
   config.gridDim = dim3(unsigned(cluster * clusters));
@@ -283,10 +286,10 @@ cudaError_t launch_shape(const BatchDesc& desc, int cluster, int clusters, cudaS
   attribute[0].val.clusterDim.z = 1;
   config.attrs = attribute;
   config.numAttrs = 1;
-  return cudaLaunchKernelEx(&config, batch_solve_kernel<Threads>, desc);
+  return cudaLaunchKernelEx(&config, batch_solve_kernel<Threads, Lean>, desc);
 }
 
-template <int Threads>
+template <int Threads, bool Lean>
 int resident_clusters(int cluster) {
   cudaLaunchConfig_t config{};
   config.gridDim = dim3(unsigned(cluster));
@@ -299,7 +302,7 @@ int resident_clusters(int cluster) {
   config.attrs = attribute;
   config.numAttrs = 1;
   int count = 0;
-  if (cudaOccupancyMaxActiveClusters(&count, batch_solve_kernel<Threads>, &config) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveClusters(&count, batch_solve_kernel<Threads, Lean>, &config) != cudaSuccess) {
     cudaGetLastError();
     return 0;
   }
@@ -320,13 +323,24 @@ __global__ void colony_row_keys_kernel(const uint2* __restrict__ slots, std::uin
 }  // namespace
 
 int batch_resident_clusters(BatchShape shape) {
-  return shape.threads == 512 ? resident_clusters<512>(shape.cluster) : resident_clusters<256>(shape.cluster);
+  if (shape.lean) {
+    return shape.threads == 512 ? resident_clusters<512, true>(shape.cluster)
+                                : resident_clusters<256, true>(shape.cluster);
+  }
+  return shape.threads == 512 ? resident_clusters<512, false>(shape.cluster)
+                              : resident_clusters<256, false>(shape.cluster);
 }
 
 int launch_batch_solve(const BatchDesc& desc, BatchShape shape, int clusters, cudaStream_t stream) {
   if (clusters <= 0 || desc.colonies == 0) return int(cudaSuccess);
-  const cudaError_t e = shape.threads == 512 ? launch_shape<512>(desc, shape.cluster, clusters, stream)
-                                             : launch_shape<256>(desc, shape.cluster, clusters, stream);
+  cudaError_t e;
+  if (shape.lean) {
+    e = shape.threads == 512 ? launch_shape<512, true>(desc, shape.cluster, clusters, stream)
+                             : launch_shape<256, true>(desc, shape.cluster, clusters, stream);
+  } else {
+    e = shape.threads == 512 ? launch_shape<512, false>(desc, shape.cluster, clusters, stream)
+                             : launch_shape<256, false>(desc, shape.cluster, clusters, stream);
+  }
   count_launch();
   return int(e);
 }

@@ -50,6 +50,7 @@ struct BatchDesc {
 struct BatchShape {
   int cluster;  // 1, 2, 4 or 8
   int threads;  // 256 or 512
+  bool lean;    // 64-register form (one gather in flight per thread, more resident warps)
 };
 
 // Clusters of `shape` that fit on the device at once (0 if none).

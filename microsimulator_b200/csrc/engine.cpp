@@ -346,6 +346,7 @@ struct msb_context {
   msb::DBuf<std::uint16_t> features;
   msb::DBuf<float> net_outputs;
   msb::DBuf<std::uint32_t> knn_keys, knn_values, knn_counts, knn_offsets, knn_bounds;
+  msb::DBuf<float2> knn_centres;
   bool has_guess = false;
   std::uint32_t guess_cells = 0;
   float guess_dt = 0.0f;
@@ -368,7 +369,7 @@ struct msb_context {
   std::vector<std::uint64_t> colony_iterations;
   std::vector<float> colony_max_overlap;
   std::vector<std::uint32_t> colony_rows_at_accept;
-  msb::BatchShape batch_shape{4, 256};
+  msb::BatchShape batch_shape{4, 256, false};
   int batch_clusters = 0;
   bool batch_tuned = false;
   float box_scale = 1.0f;        // the contact search's box scale for the current call
@@ -814,9 +815,9 @@ void tune_batch(Ctx& c, const msb::BatchDesc& d) {
   check(cudaEventCreate(&start), "event");
   check(cudaEventCreate(&stop), "event");
   float best = -1.0f;
-  for (const int threads : {256, 512}) {
+  for (const bool lean : {false, true}) for (const int threads : {256, 512}) {
     for (const int cluster : {1, 2, 4, 8}) {
-      const msb::BatchShape shape{cluster, threads};
+      const msb::BatchShape shape{cluster, threads, lean};
       const int resident = batch_resident_clusters(shape);
       if (resident <= 0) continue;
       const int clusters = std::min<int>(resident, int(c.colonies));
@@ -984,11 +985,13 @@ void compute_features(Ctx& c, GeometryBuffers geometry) {
   c.knn_offsets.ensure(bins + 1ull);
   c.temp.ensure(sort_temp_words(n) + scan_temp_words(bins + 1ull) + 64);
   check(cudaMemsetAsync(c.knn_counts.p, 0, (bins + 1ull) * 4, c.stream), "memset");
-  mlp::Grid grid{x0, y0, float(1.0 / side), nx, ny, c.knn_offsets.p, c.knn_values.p};
+  c.knn_centres.ensure(n);
+  mlp::Grid grid{x0, y0, float(1.0 / side), nx, ny, c.knn_offsets.p, c.knn_values.p, c.knn_centres.p};
   mlp::launch_bin_keys(n, geometry.pos_len, grid, c.knn_keys.p, c.knn_values.p, c.knn_counts.p, c.stream);
   exclusive_scan(c.knn_counts.p, c.knn_offsets.p, bins + 1ull, c.temp.p, c.stream);
   const int bits = std::max(1, int(std::bit_width(bins)));
   radix_sort_pairs(c.knn_keys.p, c.knn_values.p, n, bits, c.temp.p, c.stream);
+  mlp::launch_sorted_centres(n, geometry.pos_len, c.knn_values.p, c.knn_centres.p, c.stream);
   mlp::launch_features(n, geometry.pos_len, geometry.dir_rad, grid, c.features.p, c.stream);
 }
 
@@ -1896,12 +1899,14 @@ int msb_tune_batch(msb_context* context) {
   return MSB_OK;
 }
 
-int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, float* box_scale) {
-  if (context == nullptr || cluster == nullptr || threads == nullptr || box_scale == nullptr) {
+int msb_batch_tuning(const msb_context* context, uint32_t* cluster, uint32_t* threads, uint32_t* lean,
+                     float* box_scale) {
+  if (context == nullptr || cluster == nullptr || threads == nullptr || lean == nullptr || box_scale == nullptr) {
     return MSB_ERR_INVALID_ARGUMENT;
   }
   *cluster = std::uint32_t(context->batch_shape.cluster);
   *threads = std::uint32_t(context->batch_shape.threads);
+  *lean = context->batch_shape.lean ? 1u : 0u;
   *box_scale = context->batch_box_scale;
   return MSB_OK;
 }

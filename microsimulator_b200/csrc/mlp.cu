@@ -111,6 +111,14 @@ __device__ __forceinline__ std::uint32_t bin_of(const Grid& g, float x, float y,
   return by * g.nx + bx;
 }
 
+__global__ void sorted_centres_kernel(std::uint32_t n, const float4* __restrict__ pos_len,
+                                      const std::uint32_t* __restrict__ slots, float2* __restrict__ centres) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const float4 p = pos_len[slots[k]];
+    centres[k] = make_float2(p.x, p.y);
+  }
+}
+
 __global__ void bin_keys_kernel(std::uint32_t n, const float4* __restrict__ pos_len, Grid grid,
                                 std::uint32_t* __restrict__ keys, std::uint32_t* __restrict__ values,
                                 std::uint32_t* __restrict__ counts) {
@@ -129,7 +137,9 @@ __global__ void bin_keys_kernel(std::uint32_t n, const float4* __restrict__ pos_
 __global__ void __launch_bounds__(kThreads) features_kernel(std::uint32_t n, const float4* __restrict__ pos_len,
                                                              const float4* __restrict__ dir_rad, Grid grid,
                                                              std::uint16_t* __restrict__ features) {
-  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
+  // Cells in bin order, so that a warp's cells search the same bins.
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const std::uint32_t s = grid.slots[k];
     const float4 p = pos_len[s];
     const float4 d = dir_rad[s];
     float ax = d.x, ay = d.y;
@@ -157,10 +167,10 @@ __global__ void __launch_bounds__(kThreads) features_kernel(std::uint32_t n, con
         const int x = int(bx) + ox;
         if (x < 0 || x >= int(grid.nx)) continue;
         const std::uint32_t bin = std::uint32_t(y) * grid.nx + std::uint32_t(x);
-        for (std::uint32_t k = grid.offsets[bin]; k < grid.offsets[bin + 1]; ++k) {
-          const std::uint32_t o = grid.slots[k];
+        for (std::uint32_t m = grid.offsets[bin]; m < grid.offsets[bin + 1]; ++m) {
+          const std::uint32_t o = grid.slots[m];
           if (o == s) continue;
-          const float4 q = pos_len[o];
+          const float2 q = grid.centres[m];
           const float dx = q.x - p.x, dy = q.y - p.y;
           const float d2 = dx * dx + dy * dy;
           if (d2 > best_d[kNeighbours - 1] || (d2 == best_d[kNeighbours - 1] && o > best_s[kNeighbours - 1])) continue;
@@ -496,6 +506,13 @@ void launch_bin_keys(std::uint32_t n, const float4* pos_len, Grid grid, std::uin
                      std::uint32_t* counts, cudaStream_t stream) {
   if (n == 0) return;
   bin_keys_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, pos_len, grid, keys, values, counts);
+  count_launch();
+}
+
+void launch_sorted_centres(std::uint32_t n, const float4* pos_len, const std::uint32_t* slots, float2* centres,
+                           cudaStream_t stream) {
+  if (n == 0) return;
+  sorted_centres_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, pos_len, slots, centres);
   count_launch();
 }
 

@@ -48,6 +48,7 @@ struct Grid {
   std::uint32_t nx, ny;
   const std::uint32_t* offsets;  // nx * ny + 1
   const std::uint32_t* slots;    // cells sorted by bin
+  const float2* centres;         // their centres (x, y), in the same order
 };
 
 // Bounds of the cell centres: out[0..3] = min x, min y, max x, max y (as
@@ -57,6 +58,9 @@ void launch_centre_bounds(std::uint32_t n, const float4* pos_len, std::uint32_t*
 // Bin keys of each cell and per-bin counts (counts zeroed by the caller).
 void launch_bin_keys(std::uint32_t n, const float4* pos_len, Grid grid, std::uint32_t* keys, std::uint32_t* values,
                      std::uint32_t* counts, cudaStream_t stream);
+// The bin-sorted copy of the centres (grid.centres) from grid.slots.
+void launch_sorted_centres(std::uint32_t n, const float4* pos_len, const std::uint32_t* slots, float2* centres,
+                           cudaStream_t stream);
 // Features of every cell, n x kInput bf16 (as uint16 bits), zero padded.
 void launch_features(std::uint32_t n, const float4* pos_len, const float4* dir_rad, Grid grid,
                      std::uint16_t* features, cudaStream_t stream);
