@@ -247,17 +247,28 @@ __global__ void broad_phase_kernel(GeometryView g, const double* __restrict__ bo
     const float4 my_hi = sorted_hi[k];
     const std::uint32_t a = __float_as_uint(my_lo.w);
     if (fill && slab != nullptr && counts[rank[a]] <= std::uint32_t(kLocalPartners)) continue;
+    const std::uint32_t colony = g.colony != nullptr ? g.colony[a] : 0u;
+    if (g.colony_active != nullptr && g.colony_active[colony] == 0u) {
+      if (!fill) counts[rank[a]] = 0;  // a settled colony of a batch: no partners this round
+      continue;
+    }
     const std::uint64_t id = sorted_id[k];
     double box[6];
 #pragma unroll
     for (int q = 0; q < 6; ++q) box[q] = bounds[6 * std::uint64_t(a) + q];
     std::int64_t at[3];
-    box_of(box, grid, at, g.colony != nullptr ? g.colony[a] : 0u);
+    box_of(box, grid, at, colony);
     std::int64_t first[3], last[3];
 #pragma unroll
     for (int q = 0; q < 3; ++q) {
       first[q] = at[q] == 0 ? 0 : at[q] - 1;
       last[q] = smin(std::int64_t(grid.dims[q]) - 1, at[q] + 1);
+    }
+    if (grid.colony_stride > 0) {
+      // Only the colony's own z boxes hold its cells.
+      const std::int64_t own = std::int64_t(colony) * std::int64_t(grid.colony_stride);
+      first[2] = smax(first[2], own);
+      last[2] = smin(last[2], own + std::int64_t(grid.colony_stride) - 3);
     }
     const std::uint32_t base = fill ? offsets[rank[a]] : 0;
     std::uint32_t found = 0;

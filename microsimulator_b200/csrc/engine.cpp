@@ -361,7 +361,7 @@ struct msb_context {
   std::uint32_t colonies = 0;
   std::vector<std::uint32_t> host_colony_offsets;
   msb::DBuf<std::uint32_t> colony_offsets, colony_of_slot, colony_order, colony_overlap, colony_rows,
-      colony_row_counts, colony_row_offsets, batch_next;
+      colony_row_counts, colony_row_offsets, batch_next, colony_active, colony_flagged;
   msb::DBuf<float> colony_drag, colony_stiffness, colony_tolerance, colony_solve_tolerance, colony_slack,
       batch_saved;
   msb::DBuf<msb::ColonyState> colony_state;
@@ -476,14 +476,16 @@ std::uint32_t read_u32(Ctx& c, const std::uint32_t* device_ptr) {
 }
 
 GeometryView view_of(Ctx& c, Geometry& g) {
-  return {g.pos_len.p, g.dir_rad.p, c.ids.p, c.n, c.colonies > 0 ? c.colony_of_slot.p : nullptr};
+  return {g.pos_len.p, g.dir_rad.p, c.ids.p, c.n, c.colonies > 0 ? c.colony_of_slot.p : nullptr,
+          c.colonies > 0 ? c.colony_active.p : nullptr};
 }
 
 // ---- cells ---------------------------------------------------------------
 
 Colonies colonies_of(Ctx& c) {
   if (c.colonies == 0) return {};
-  return {c.colony_of_slot.p, c.colony_drag.p, c.colony_stiffness.p, c.colony_overlap.p, c.colony_slack.p};
+  return {c.colony_of_slot.p,   c.colony_drag.p,  c.colony_stiffness.p,
+          c.colony_overlap.p,   c.colony_slack.p, c.colony_flagged.p};
 }
 
 void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
@@ -918,7 +920,10 @@ Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_const
   c.flag_offsets.ensure(o.candidates + 1ull);
   reset_scalars(c);
   check(cudaMemsetAsync(c.flags.p + o.candidates, 0, 4, c.stream), "memset");
-  if (c.colonies > 0) check(cudaMemsetAsync(c.colony_overlap.p, 0, c.colonies * 4ull, c.stream), "memset");
+  if (c.colonies > 0) {
+    launch_colony_reset_overlap(c.colonies, c.colony_active.p, c.colony_overlap.p, c.stream);
+    check(cudaMemsetAsync(c.colony_flagged.p, 0, c.colonies * 4ull, c.stream), "memset");
+  }
   launch_recheck(c.found.p, o.candidates, c.rows.keyed(), c.slack.p, p.wall_stiffness, p.contact_stiffness,
                  c.flags.p, c.scalars.p + kOverlapBits, c.stream, colonies_of(c));
   c.temp.ensure(scan_temp_words(o.candidates + 1ull) + 64);
@@ -929,6 +934,10 @@ Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_const
   read_scalars(c);
   o.overlapping = c.host_scalars[kScalarCount + 4];
   o.max_overlap = bits_to_float(c.host_scalars[kOverlapBits]);
+  // A batch's colonies with nothing flagged leave the following rounds'
+  // searches: their rows are final, their solves converge at once and their
+  // moves repeat.
+  if (c.colonies > 0 && o.overlapping > 0) launch_colony_refine(c.colonies, c.colony_flagged.p, c.colony_active.p, c.stream);
   return o;
 }
 
@@ -1036,6 +1045,10 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
                         const msb_constraint_contact_parameters& wp, bool probe, std::uint64_t& iterations) {
   const std::uint32_t n = c.n;
   c.has_drift = false;  // the stepper's bodies carry no drift (flow drift is not supported)
+  if (c.colonies > 0) {
+    // Every colony takes part in the substep's first search and test.
+    check(cudaMemsetAsync(c.colony_active.p, 0xFF, c.colonies * 4ull, c.stream), "memset");
+  }
   c.body_a.ensure(n);
   c.body_b.ensure(n);
   c.drift_a.ensure(n);
@@ -1827,6 +1840,9 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     c.colony_solve_tolerance.ensure(colony_count);
     c.colony_overlap.ensure(colony_count);
     c.colony_slack.ensure(colony_count);
+    c.colony_active.ensure(colony_count);
+    c.colony_flagged.ensure(colony_count);
+    check(cudaMemsetAsync(c.colony_active.p, 0xFF, colony_count * 4ull, c.stream), "memset");
     c.colony_state.ensure(colony_count);
     c.batch_next.ensure(1);
     c.colony_of_slot.ensure(std::max<std::uint32_t>(c.n, 1));

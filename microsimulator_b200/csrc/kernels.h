@@ -43,6 +43,8 @@ struct GeometryView {
   // gives every colony its own range of z boxes, so that no two colonies'
   // cells are ever candidates of one another.  Null for one system.
   const std::uint32_t* colony = nullptr;
+  // Colonies still searched in a batch's refinement round (null: all).
+  const std::uint32_t* colony_active = nullptr;
 };
 
 // One contact of a cell with a cell (s2 valid) or with a constraint (s2 =

@@ -356,6 +356,7 @@ __global__ void recheck_kernel(const Touch* __restrict__ touches, std::uint32_t 
     const float compliance = 1.0f / (wall ? wall_stiffness : contact_stiffness);
     const float allowed = slack + force * compliance;
     flags[k] = t.sep < -allowed ? 1u : 0u;
+    if (flags[k] != 0u && colonies.flagged != nullptr) atomicAdd(colonies.flagged + colony, 1u);
   }
 }
 
@@ -379,6 +380,20 @@ __global__ void colony_slack_kernel(std::uint32_t colonies, const std::uint32_t*
   for (std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < colonies; c += gridDim.x * blockDim.x) {
     const float starting = __uint_as_float(overlap_bits[c]);
     slack[c] = tolerance[c] + smax(0.0f, starting - recovery);
+  }
+}
+
+__global__ void colony_refine_kernel(std::uint32_t colonies, const std::uint32_t* __restrict__ flagged,
+                                     std::uint32_t* __restrict__ active) {
+  for (std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < colonies; c += gridDim.x * blockDim.x) {
+    active[c] = (active[c] != 0u && flagged[c] != 0u) ? 1u : 0u;
+  }
+}
+
+__global__ void colony_reset_overlap_kernel(std::uint32_t colonies, const std::uint32_t* __restrict__ active,
+                                            std::uint32_t* __restrict__ overlap_bits) {
+  for (std::uint32_t c = blockIdx.x * blockDim.x + threadIdx.x; c < colonies; c += gridDim.x * blockDim.x) {
+    if (active[c] != 0u) overlap_bits[c] = 0u;
   }
 }
 
@@ -595,6 +610,20 @@ void launch_colony_slack(std::uint32_t colonies, const std::uint32_t* overlap_bi
   if (colonies == 0) return;
   colony_slack_kernel<<<grid_for(colonies, kThreads), kThreads, 0, stream>>>(colonies, overlap_bits, tolerance,
                                                                              recovery, slack);
+  count_launch();
+}
+
+void launch_colony_refine(std::uint32_t colonies, const std::uint32_t* flagged, std::uint32_t* active,
+                          cudaStream_t stream) {
+  if (colonies == 0) return;
+  colony_refine_kernel<<<grid_for(colonies, kThreads), kThreads, 0, stream>>>(colonies, flagged, active);
+  count_launch();
+}
+
+void launch_colony_reset_overlap(std::uint32_t colonies, const std::uint32_t* active, std::uint32_t* overlap_bits,
+                                 cudaStream_t stream) {
+  if (colonies == 0) return;
+  colony_reset_overlap_kernel<<<grid_for(colonies, kThreads), kThreads, 0, stream>>>(colonies, active, overlap_bits);
   count_launch();
 }
 

@@ -27,7 +27,15 @@ struct Colonies {
   const float* stiffness;
   std::uint32_t* overlap_bits;
   const float* slack;
+  std::uint32_t* flagged;  // per colony: touches the overlap test flagged
 };
+// Between refinement rounds of a batch: colonies whose overlap test flagged
+// nothing leave the search (active = 0) and keep their overlap record;
+// the others reset their record for the next test.
+void launch_colony_refine(std::uint32_t colonies, const std::uint32_t* flagged, std::uint32_t* active,
+                          cudaStream_t stream);
+void launch_colony_reset_overlap(std::uint32_t colonies, const std::uint32_t* active, std::uint32_t* overlap_bits,
+                                 cudaStream_t stream);
 
 // Packs SoA cell arrays (device pointers) into float4 geometry, checking
 // what WorldState::validate checks.  status: kStatusGeometry on bad input.
