@@ -330,6 +330,8 @@ def sweep_arm(args, backend, local, rank, dist):
         total_ms += ms
         cell_steps += n
         iterations += int(colonies["iterations"].sum())
+        converged = int((colonies["status"] == 0).sum())
+        deepest = float(colonies["max_overlap"].max()) if len(colonies) else 0.0
         for name, value in backend.last_step_phases().items():
             phases[name] += value / args.steps
     total_ms = replicas.max_over_ranks(total_ms, dist, device)
@@ -364,6 +366,8 @@ def sweep_arm(args, backend, local, rank, dist):
         "ms_per_step": total_ms / args.steps,
         "bb_iterations_per_step_summed_over_colonies": iterations / args.steps,
         "phase_ms_per_step": phases,
+        "colonies_converged_last_step": f"{converged} of {len(batch)} on this rank",
+        "deepest_overlap_last_step_um": deepest,
         "tuning": tuning,
         "one_call_per_colony": {"value": sequential_cells / (sequential_ms * 1e-3), "unit": "cell-steps/s",
                                 "ms_per_step": sequential_ms, "timing": "host wall clock around each device call"},

@@ -489,7 +489,7 @@ typedef struct msb_colony_report {
   float max_overlap;   /* deepest overlap at the accepted geometry */
   uint32_t rows;       /* rows of the colony's last solved system */
   uint32_t cells;
-  uint32_t reserved;
+  uint32_t status;     /* msb_solve_status of the colony's last solve */
 } msb_colony_report;
 
 int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* cells, const uint32_t* colony_cells,

@@ -224,7 +224,7 @@ class ColonyParameters(ctypes.Structure):
 
 # numpy views of the record types, for bulk conversion.
 COLONY_REPORT_DTYPE = np.dtype([("iterations", "<u8"), ("max_overlap", "<f4"), ("rows", "<u4"), ("cells", "<u4"),
-                                ("reserved", "<u4")])
+                                ("status", "<u4")])
 
 CELL_CONTACT_DTYPE = np.dtype(
     [

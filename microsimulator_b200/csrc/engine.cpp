@@ -367,6 +367,7 @@ struct msb_context {
   msb::DBuf<msb::ColonyState> colony_state;
   std::vector<msb::ColonyState> host_colony_state;
   std::vector<std::uint64_t> colony_iterations;
+  std::vector<std::uint32_t> colony_status;
   std::vector<float> colony_max_overlap;
   std::vector<std::uint32_t> colony_rows_at_accept;
   msb::BatchShape batch_shape{4, 256, false};
@@ -878,6 +879,7 @@ SolveOutcome solve_batch(Ctx& c, float dt, const msb_growth_load_response& growt
     const auto& st = c.host_colony_state[i];
     if (st.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
     c.colony_iterations[i] += st.iterations;
+    c.colony_status[i] = st.status;
     out.iterations = std::max(out.iterations, st.iterations);
     residual = std::max(residual, st.residual);
     if (st.status == MSB_SOLVE_BREAKDOWN) {
@@ -1858,6 +1860,7 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     launch_colony_of_slot(colony_count, c.colony_offsets.p, c.n, c.colony_of_slot.p, c.stream);
     c.has_memory = c.has_memory && (c.warm_start_mode & kWarmCarry) != 0;
     c.colony_iterations.assign(colony_count, 0);
+    c.colony_status.assign(colony_count, MSB_SOLVE_CONVERGED);
     c.colony_max_overlap.assign(colony_count, 0.0f);
     c.colony_rows_at_accept.assign(colony_count, 0);
     if (c.tune_search && c.n > 1) {
@@ -1903,7 +1906,8 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     *report = outcome.report;
     for (std::uint32_t i = 0; i < colony_count; ++i) {
       colony_reports[i] = {c.colony_iterations[i], c.colony_max_overlap[i],
-                           i < c.colony_rows_at_accept.size() ? c.colony_rows_at_accept[i] : 0u, colony_cells[i]};
+                           i < c.colony_rows_at_accept.size() ? c.colony_rows_at_accept[i] : 0u, colony_cells[i],
+                           c.colony_status[i]};
     }
   });
 }

@@ -71,6 +71,8 @@ def test_each_colony_steps_as_it_would_alone(backend):
             assert spread < 0.05, (k, spread)
         assert np.all(np.isfinite(w.geometry()))
         assert colonies["iterations"][k] > 0 or r.iterations == 0
+        # Each colony's last solve converged to its own tolerance.
+        assert colonies["status"][k] == 0
 
 
 def SIZES_after(worlds):
