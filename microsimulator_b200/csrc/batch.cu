@@ -139,11 +139,6 @@ __device__ void block_reduce(double (&v)[5], double (&red)[5][Threads / 32], dou
   }
 }
 
-struct Decision {
-  float step;
-  std::uint32_t proceed;
-};
-
 // Two forms, picked by the autotuner: Lean = false keeps 4 incidence
 // entries' gathers in flight per thread (128 registers); Lean = true one
 // (64 registers), for twice the resident warps.
@@ -155,7 +150,6 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
   const std::uint32_t size = cluster.num_blocks();
   __shared__ double red[5][Threads / 32];
   __shared__ double part[6];  // this CTA's reduced values (5) and its diagonal bound
-  __shared__ Decision decision;
   __shared__ std::uint32_t claimed;
   __shared__ float bound_part;
   const std::uint32_t tid = rank * Threads + threadIdx.x;
@@ -200,10 +194,14 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
     __threadfence();
     cluster.sync();
 
-    // Rank 0 keeps the colony's state; the others read its decisions.
+    // Every CTA's thread 0 reads all ranks' partials in rank order and takes
+    // the same decision (the same reads in the same order), so no CTA waits
+    // for another's decision: two cluster barriers per iteration.
+    __shared__ float step_s;
+    __shared__ std::uint32_t proceed_s;
     float step = 0.0f, residual = 0.0f, colony_bound = 0.0f;
     std::uint32_t iterations = 0, status = MSB_SOLVE_ITERATION_LIMIT;
-    if (rank == 0 && threadIdx.x == 0) {
+    if (threadIdx.x == 0) {
       double total_residual = 0.0, finite = 1.0, b = 0.0;
       for (std::uint32_t r = 0; r < size; ++r) {
         const double* p = cluster.map_shared_rank(part, r);
@@ -226,21 +224,22 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
         step = 1.0f / colony_bound;
         proceed = d.max_iterations > 0 ? 1u : 0u;
       }
-      decision = {step, proceed};
+      step_s = step;
+      proceed_s = proceed;
     }
-    cluster.sync();
-    Decision now = *cluster.map_shared_rank(&decision, 0);
+    __syncthreads();
 
-    while (now.proceed != 0) {
-      colony_body_pass<kBatch>(d, b0, b1, tid, stride, true, now.step);
+    while (proceed_s != 0) {
+      const float alpha = step_s;
+      colony_body_pass<kBatch>(d, b0, b1, tid, stride, true, alpha);
       __threadfence();
       cluster.sync();
-      s = colony_row_pass(d, r0, r1, tid, stride, true, now.step);
+      s = colony_row_pass(d, r0, r1, tid, stride, true, alpha);
       double w[5] = {s.ss, s.sy, s.yy, double(s.residual), s.finite ? 1.0 : 0.0};
       block_reduce<Threads>(w, red, part);
       __threadfence();
       cluster.sync();
-      if (rank == 0 && threadIdx.x == 0) {
+      if (threadIdx.x == 0) {
         double t[5] = {0.0, 0.0, 0.0, 0.0, 1.0};
         for (std::uint32_t r = 0; r < size; ++r) {
           const double* p = cluster.map_shared_rank(part, r);
@@ -262,13 +261,14 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
           status = MSB_SOLVE_ITERATION_LIMIT;
           proceed = iterations < d.max_iterations ? 1u : 0u;
         }
-        decision = {step, proceed};
+        step_s = step;
+        proceed_s = proceed;
       }
-      cluster.sync();
-      now = *cluster.map_shared_rank(&decision, 0);
+      __syncthreads();
     }
     if (rank == 0 && threadIdx.x == 0) d.state[colony] = {step, residual, colony_bound, iterations, status};
-    cluster.sync();  // every CTA has read this colony's last decision before rank 0 claims the next
+    // The next claim's two barriers order every remote read of this colony's
+    // partials before any CTA writes them again or exits.
   }
 }
 
