@@ -164,6 +164,10 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
     cluster.sync();
     if (slot >= d.colonies) break;
     const std::uint32_t colony = d.order[slot];
+    if (d.active != nullptr && d.active[colony] == 0u) {
+      if (rank == 0 && threadIdx.x == 0) d.state[colony].iterations = 0;
+      continue;
+    }
     const std::uint32_t r0 = d.row_offsets[colony], r1 = d.row_offsets[colony + 1];
     const std::uint32_t b0 = d.cell_offsets[colony], b1 = d.cell_offsets[colony + 1];
     const float tolerance = d.tolerance[colony];

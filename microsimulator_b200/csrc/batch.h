@@ -33,6 +33,10 @@ struct BatchDesc {
   const std::uint32_t* row_offsets;   // colonies + 1
   const std::uint32_t* cell_offsets;  // colonies + 1: a colony's bodies are a slot range
   const std::uint32_t* order;         // colonies in the order the queue hands them out
+  // Colonies to solve (null: all).  A colony left out keeps its multipliers
+  // and response from its last solve and reports 0 iterations: the stepper
+  // leaves out colonies whose rows are unchanged since a converged solve.
+  const std::uint32_t* active;
   const float* tolerance;             // per colony
   ColonyState* state;                 // per colony
   std::uint32_t* next;                // the queue's counter, zero at launch

@@ -787,6 +787,7 @@ msb::BatchDesc batch_desc(Ctx& c, float dt, const msb_growth_load_response& grow
   d.row_offsets = c.colony_row_offsets.p;
   d.cell_offsets = c.colony_offsets.p;
   d.order = c.colony_order.p;
+  d.active = c.colony_active.p;
   d.tolerance = c.colony_solve_tolerance.p;
   d.state = c.colony_state.p;
   d.next = c.batch_next.p;
