@@ -448,6 +448,11 @@ def main():
     e2e = None
     if not args.no_e2e:
         world = snapshot.copy()
+        # One untimed host-buffer call first (from a copy): it sizes the
+        # context's pinned staging buffers and starts its copy threads.
+        warm = snapshot.copy()
+        divide(warm, args.warmup - 1, args.seed + rank)
+        backend.advance_contact_dynamics(warm, None, DT, dyn)
         e2e_s = 0.0
         e2e_cells = 0
         h2d = d2h = 0

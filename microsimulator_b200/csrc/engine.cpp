@@ -12,13 +12,16 @@
 #include <array>
 #include <atomic>
 #include <bit>
+#include <condition_variable>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <span>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -294,6 +297,124 @@ void require_multipliers(const float* m, std::uint64_t n) {
 }  // namespace
 }  // namespace msb
 
+namespace msb {
+
+// Copies between a caller's pageable host arrays and pinned staging memory,
+// split over a few threads: the device side of a host-buffer call is then
+// one DMA per array at full PCIe speed, and the host side runs in parallel
+// (pageable cudaMemcpy goes through the driver's single bounce buffer).
+class HostCopies {
+ public:
+  struct Job {
+    void* dst;
+    const void* src;
+    std::size_t bytes;
+  };
+
+  HostCopies() {
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned helpers = std::min(7u, hw > 1 ? hw - 1 : 0u);
+    for (unsigned t = 0; t < helpers; ++t) threads_.emplace_back([this] { serve(); });
+  }
+  HostCopies(const HostCopies&) = delete;
+  HostCopies& operator=(const HostCopies&) = delete;
+  ~HostCopies() {
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      stop_ = true;
+    }
+    wake_.notify_all();
+    for (auto& t : threads_) t.join();
+  }
+
+  // Runs every job (split into chunks) on the pool and this thread; returns
+  // when all are done.
+  void run(const std::vector<Job>& jobs) {
+    chunks_.clear();
+    constexpr std::size_t kChunk = std::size_t(1) << 21;
+    for (const auto& j : jobs) {
+      for (std::size_t at = 0; at < j.bytes; at += kChunk) {
+        const std::size_t len = std::min(kChunk, j.bytes - at);
+        chunks_.push_back({static_cast<char*>(j.dst) + at, static_cast<const char*>(j.src) + at, len});
+      }
+    }
+    if (chunks_.empty()) return;
+    {
+      std::lock_guard<std::mutex> lock(mutex_);
+      next_.store(0);
+      busy_ = threads_.size();
+      ++generation_;
+    }
+    wake_.notify_all();
+    work();
+    std::unique_lock<std::mutex> lock(mutex_);
+    done_.wait(lock, [this] { return busy_ == 0; });
+  }
+
+ private:
+  void work() {
+    for (;;) {
+      const std::size_t k = next_.fetch_add(1);
+      if (k >= chunks_.size()) return;
+      std::memcpy(chunks_[k].dst, chunks_[k].src, chunks_[k].bytes);
+    }
+  }
+  void serve() {
+    std::uint64_t seen = 0;
+    for (;;) {
+      {
+        std::unique_lock<std::mutex> lock(mutex_);
+        wake_.wait(lock, [&] { return stop_ || generation_ != seen; });
+        if (stop_) return;
+        seen = generation_;
+      }
+      work();
+      {
+        std::lock_guard<std::mutex> lock(mutex_);
+        if (--busy_ == 0) done_.notify_all();
+      }
+    }
+  }
+
+  std::vector<std::thread> threads_;
+  std::vector<Job> chunks_;
+  std::atomic<std::size_t> next_{0};
+  std::mutex mutex_;
+  std::condition_variable wake_, done_;
+  std::size_t busy_ = 0;
+  std::uint64_t generation_ = 0;
+  bool stop_ = false;
+};
+
+// Pinned host memory grown on demand.
+struct PinnedBuffer {
+  unsigned char* p = nullptr;
+  std::size_t cap = 0;
+  PinnedBuffer() = default;
+  PinnedBuffer(const PinnedBuffer&) = delete;
+  PinnedBuffer& operator=(const PinnedBuffer&) = delete;
+  ~PinnedBuffer() { release(); }
+  void release() {
+    if (p != nullptr) cudaFreeHost(p);
+    p = nullptr;
+    cap = 0;
+  }
+  unsigned char* ensure(std::size_t bytes) {
+    if (bytes > cap) {
+      release();
+      const std::size_t c = std::bit_ceil(std::max<std::size_t>(bytes + bytes / 4, 1 << 20));
+      if (cudaMallocHost(reinterpret_cast<void**>(&p), c) != cudaSuccess) {
+        p = nullptr;
+        throw std::runtime_error("cudaMallocHost failed for staging memory");
+      }
+      cap = c;
+    }
+    return p;
+  }
+};
+
+}  // namespace msb
+
 struct msb_context {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -387,6 +508,11 @@ struct msb_context {
   msb::DBuf<std::uint32_t> scalars;
   std::uint32_t* host_scalars = nullptr;
   msb::SolveDesc* host_desc = nullptr;
+
+  // host-buffer calls: pinned staging both ways and the host-side copy pool
+  std::unique_ptr<msb::HostCopies> copies;
+  msb::PinnedBuffer upload, download;
+  std::vector<msb::HostCopies::Job> pending;  // download copies to run after the stream syncs
 
   // phase timing of the last step: events at phase boundaries
   std::vector<cudaEvent_t> phase_events;
@@ -489,6 +615,27 @@ Colonies colonies_of(Ctx& c) {
           c.colony_overlap.p,   c.colony_slack.p, c.colony_flagged.p};
 }
 
+msb::HostCopies& host_copies(Ctx& c) {
+  if (!c.copies) c.copies = std::make_unique<msb::HostCopies>();
+  return *c.copies;
+}
+
+// A device-to-host copy into the caller's pageable `dst` through the pinned
+// download buffer: the DMA is queued now, the host copy waits in c.pending
+// for the stream's next sync (flush_downloads).  `at` is the running offset.
+void stage_download(Ctx& c, void* dst, const void* device_src, std::size_t bytes, std::size_t& at) {
+  unsigned char* slot = c.download.p + at;
+  check(cudaMemcpyAsync(slot, device_src, bytes, cudaMemcpyDeviceToHost, c.stream), "copy back");
+  c.pending.push_back({dst, slot, bytes});
+  at += (bytes + 255) & ~std::size_t(255);
+}
+
+void flush_downloads(Ctx& c) {
+  if (c.pending.empty()) return;
+  host_copies(c).run(c.pending);
+  c.pending.clear();
+}
+
 void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
   if (cells.count >= 0xFFFFFFF0ull) throw std::overflow_error("cell count exceeds the slot index space");
   if (cells.count > 0 && (cells.ids == nullptr || cells.position_x == nullptr || cells.position_y == nullptr ||
@@ -500,26 +647,48 @@ void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
   c.n = std::uint32_t(cells.count);
   const std::size_t n = c.n;
   if (n == 0) return;
-  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
   c.ids.ensure(n);
   c.growth.ensure(n);
   c.fixed.ensure(n);
-  check(cudaMemcpyAsync(c.ids.p, cells.ids, n * 8, kind, c.stream), "copy ids");
   const float* src[8] = {cells.position_x,  cells.position_y,  cells.position_z, cells.direction_x,
                          cells.direction_y, cells.direction_z, cells.lengths,    cells.radii};
+  std::vector<msb::HostCopies::Job> uploads;  // (device destination, caller's source, bytes)
+  uploads.push_back({c.ids.p, cells.ids, n * 8});
   for (int k = 0; k < 8; ++k) {
     c.staging[k].ensure(n);
-    check(cudaMemcpyAsync(c.staging[k].p, src[k], n * 4, kind, c.stream), "copy cells");
+    uploads.push_back({c.staging[k].p, src[k], n * 4});
   }
   if (cells.growth_rates != nullptr) {
-    check(cudaMemcpyAsync(c.growth.p, cells.growth_rates, n * 4, kind, c.stream), "copy growth");
+    uploads.push_back({c.growth.p, cells.growth_rates, n * 4});
   } else {
     check(cudaMemsetAsync(c.growth.p, 0, n * 4, c.stream), "memset");
   }
   if (cells.fixed != nullptr) {
-    check(cudaMemcpyAsync(c.fixed.p, cells.fixed, n, kind, c.stream), "copy fixed");
+    uploads.push_back({c.fixed.p, cells.fixed, n});
   } else {
     check(cudaMemsetAsync(c.fixed.p, 0, n, c.stream), "memset");
+  }
+  if (device_pointers) {
+    for (const auto& u : uploads) {
+      check(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyDeviceToDevice, c.stream), "copy cells");
+    }
+  } else {
+    // Through pinned staging: the host side in parallel, then one DMA per array.
+    std::size_t total = 0;
+    for (const auto& u : uploads) total += (u.bytes + 255) & ~std::size_t(255);
+    unsigned char* base = c.upload.ensure(total);
+    std::vector<msb::HostCopies::Job> host;
+    std::size_t at = 0;
+    for (const auto& u : uploads) {
+      host.push_back({base + at, u.src, u.bytes});
+      at += (u.bytes + 255) & ~std::size_t(255);
+    }
+    host_copies(c).run(host);
+    at = 0;
+    for (const auto& u : uploads) {
+      check(cudaMemcpyAsync(u.dst, base + at, u.bytes, cudaMemcpyHostToDevice, c.stream), "copy cells");
+      at += (u.bytes + 255) & ~std::size_t(255);
+    }
   }
   c.state.ensure(n);
   reset_status(c);
@@ -1245,30 +1414,43 @@ StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, 
   return out;
 }
 
-void write_back(Ctx& c, msb_cell_arrays& cells, bool device_pointers) {
+// Pinned download space for a step's results with host buffers: 7 geometry
+// arrays and 5 output floats per cell, each array 256-byte aligned.
+void prepare_downloads(Ctx& c, bool device_pointers) {
+  c.pending.clear();
+  if (!device_pointers) c.download.ensure(48ull * c.n + 12 * 256);
+}
+
+void write_back(Ctx& c, msb_cell_arrays& cells, bool device_pointers, std::size_t& at) {
   const std::size_t n = c.n;
   if (n == 0) return;
   launch_unpack_cells(c.n, c.state.view(), c.staging[0].p, c.staging[1].p, c.staging[2].p, c.staging[3].p,
                       c.staging[4].p, c.staging[5].p, c.staging[6].p, c.stream);
-  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
   float* dst[7] = {cells.position_x,  cells.position_y,  cells.position_z, cells.direction_x,
                    cells.direction_y, cells.direction_z, cells.lengths};
-  for (int k = 0; k < 7; ++k) check(cudaMemcpyAsync(dst[k], c.staging[k].p, n * 4, kind, c.stream), "copy back");
+  for (int k = 0; k < 7; ++k) {
+    if (device_pointers) {
+      check(cudaMemcpyAsync(dst[k], c.staging[k].p, n * 4, cudaMemcpyDeviceToDevice, c.stream), "copy back");
+    } else {
+      stage_download(c, dst[k], c.staging[k].p, n * 4, at);
+    }
+  }
 }
 
-void write_outputs(Ctx& c, msb_contact_dynamics_outputs* outputs, bool device_pointers) {
+void write_outputs(Ctx& c, msb_contact_dynamics_outputs* outputs, bool device_pointers, std::size_t& at) {
   if (outputs == nullptr || c.n == 0) return;
   const std::size_t n = c.n;
-  const auto kind = device_pointers ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
-  if (outputs->center_velocities != nullptr) {
-    check(cudaMemcpyAsync(outputs->center_velocities, c.out_velocities.p, 12 * n, kind, c.stream), "copy out");
-  }
-  if (outputs->axial_loads != nullptr) {
-    check(cudaMemcpyAsync(outputs->axial_loads, c.out_loads.p, 4 * n, kind, c.stream), "copy out");
-  }
-  if (outputs->length_increments != nullptr) {
-    check(cudaMemcpyAsync(outputs->length_increments, c.out_increments.p, 4 * n, kind, c.stream), "copy out");
-  }
+  const auto copy = [&](void* dst, const void* src, std::size_t bytes) {
+    if (dst == nullptr) return;
+    if (device_pointers) {
+      check(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, c.stream), "copy out");
+    } else {
+      stage_download(c, dst, src, bytes, at);
+    }
+  };
+  copy(outputs->center_velocities, c.out_velocities.p, 12 * n);
+  copy(outputs->axial_loads, c.out_loads.p, 4 * n);
+  copy(outputs->length_increments, c.out_increments.p, 4 * n);
 }
 
 // Uploads a ContactSystem's records as the context's rows and bodies.
@@ -1752,10 +1934,13 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     }
     c.has_guess = false;  // a guess serves one step
     mark(c, kPhaseOutput);
-    write_back(c, *cells, device_pointers);
-    write_outputs(c, outputs, device_pointers);
+    prepare_downloads(c, device_pointers);
+    std::size_t at = 0;
+    write_back(c, *cells, device_pointers, at);
+    write_outputs(c, outputs, device_pointers, at);
     mark(c, kPhaseEnd);
     sync(c);
+    flush_downloads(c);
     collect_phases(c);
     *report = outcome.report;
   });
@@ -1899,10 +2084,13 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
       throw;
     }
     mark(c, kPhaseOutput);
-    write_back(c, *cells, device_pointers != 0);
-    write_outputs(c, outputs, device_pointers != 0);
+    prepare_downloads(c, device_pointers != 0);
+    std::size_t at = 0;
+    write_back(c, *cells, device_pointers != 0, at);
+    write_outputs(c, outputs, device_pointers != 0, at);
     mark(c, kPhaseEnd);
     sync(c);
+    flush_downloads(c);
     collect_phases(c);
     *report = outcome.report;
     for (std::uint32_t i = 0; i < colony_count; ++i) {
