@@ -439,7 +439,9 @@ uint64_t msb_mlp_activation_bytes(uint64_t rows);
 uint64_t msb_mlp_backward_scratch_bytes(uint64_t rows);
 /* outputs (rows x 3 fp32) of the network on `features`; with a non-null
  * `activations` buffer, keeps what msb_mlp_backward needs.  `stream` is a
- * cudaStream_t (null: the default stream). */
+ * cudaStream_t (null: the default stream).  Without activations (inference)
+ * the pass runs on tcgen05 with TMEM accumulators; with them (training),
+ * on mma.sync keeping each layer's activations. */
 int msb_mlp_forward(const uint16_t* weights, const float* biases, const uint16_t* features, uint64_t rows,
                     float* outputs, void* activations, void* stream);
 /* Gradients (MSB_MLP_PARAMETERS fp32, the parameters' layout) of a loss

@@ -1183,7 +1183,9 @@ void learned_guess(Ctx& c, float dt) {
   compute_features(c, c.state.view());
   c.net_outputs.ensure(3ull * std::max<std::uint32_t>(n, 1));
   c.guess.ensure(std::max<std::uint32_t>(n, 1));
-  mlp::launch_forward(c.net_weights.p, c.net_biases.p, c.features.p, n, c.net_outputs.p, nullptr, c.stream);
+  check(cudaError_t(mlp::launch_forward_tc(c.net_weights.p, c.net_biases.p, c.features.p, n, c.net_outputs.p,
+                                           c.scalars.p + kStatus, c.stream)),
+        "warm-start network");
   mlp::launch_outputs_to_guess(n, c.net_outputs.p, c.net_scale, c.state.dir_rad.p, c.guess.p, c.stream);
   check(cudaGetLastError(), "warm-start network");
   c.guess_cells = n;
@@ -1613,6 +1615,11 @@ int msb_mlp_forward(const uint16_t* weights, const float* biases, const uint16_t
   if (rows > std::numeric_limits<std::uint32_t>::max() / 2) return MSB_ERR_OVERFLOW;
   if (rows > 0 && (weights == nullptr || biases == nullptr || features == nullptr || outputs == nullptr)) {
     return MSB_ERR_INVALID_ARGUMENT;
+  }
+  if (activations == nullptr) {
+    // Inference: the tcgen05 pass.
+    return cuda_status(cudaError_t(mlp::launch_forward_tc(weights, biases, features, std::uint32_t(rows), outputs,
+                                                          nullptr, static_cast<cudaStream_t>(stream))));
   }
   mlp::launch_forward(weights, biases, features, std::uint32_t(rows), outputs, activations,
                       static_cast<cudaStream_t>(stream));

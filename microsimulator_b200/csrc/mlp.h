@@ -68,6 +68,12 @@ void launch_features(std::uint32_t n, const float4* pos_len, const float4* dir_r
 // `activations` (activation_bytes(n)), keeps H1..H3 and Z1..Z3 for backward.
 void launch_forward(const std::uint16_t* weights, const float* biases, const std::uint16_t* features,
                     std::uint32_t n, float* outputs, void* activations, cudaStream_t stream);
+// The same inference pass (no activations kept) on the tcgen05 tensor cores
+// with TMEM accumulators (mlp_tc.cu).  *error (if not null) becomes
+// kStatusIterations when a wait for the tensor cores gave up.  Returns a CUDA
+// error code.
+int launch_forward_tc(const std::uint16_t* weights, const float* biases, const std::uint16_t* features,
+                      std::uint32_t n, float* outputs, std::uint32_t* error, cudaStream_t stream);
 // Gradients of the parameters (fp32, flat layout) for output gradients
 // `output_grad` (n x 3) from the activations of launch_forward.
 void launch_backward(const std::uint16_t* weights, const std::uint16_t* features, std::uint32_t n,

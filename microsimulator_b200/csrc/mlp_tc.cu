@@ -1,0 +1,272 @@
+// The warm-start network's inference pass on the fifth-generation tensor
+// cores: tcgen05.mma with both operands in shared memory and the fp32
+// accumulator in tensor memory (TMEM).
+//
+// One CTA of 128 threads per SM works through 128-cell tiles.  Per layer:
+// thread 0 issues the layer's K/16 MMAs (M = 128 cells, N = 128 outputs, or 16
+// for the output layer), commits them to an mbarrier, and every thread (one
+// TMEM lane = one cell) reads its row of the accumulator back with
+// tcgen05.ld, adds the bias, applies GELU, rounds to bf16 and writes the row
+// into the shared-memory operand of the next layer.  Weights stay in shared
+// memory for the whole launch.
+//
+// Shared-memory operands use the canonical K-major layout without swizzle:
+// 8-row x 16-byte core matrices, rows of a core matrix 16 bytes apart, row
+// groups 128 bytes apart (the descriptor's stride byte offset) and 8-element
+// K blocks R/8 * 128 bytes apart (its leading byte offset) for R rows.
+#include <cuda_bf16.h>
+
+#include <cstdint>
+
+#include "device.cuh"
+#include "mlp.h"
+
+namespace msb::mlp {
+namespace {
+
+constexpr int kTile = 128;
+constexpr std::uint32_t kTmemColumns = 128;
+constexpr std::uint32_t kOutputRows = 16;  // the output layer's N (8 weight rows, zero padded)
+// Bytes of each shared-memory operand.
+constexpr std::uint32_t kBytesW0 = kHidden * kInput * 2;             // 24 KB
+constexpr std::uint32_t kBytesW1 = kHidden * kHidden * 2;            // 32 KB
+constexpr std::uint32_t kBytesW3 = kOutputRows * kHidden * 2;        // 4 KB
+constexpr std::uint32_t kBytesA = kTile * kHidden * 2;               // 32 KB
+constexpr std::uint32_t kOffW0 = 0;
+constexpr std::uint32_t kOffW1 = kOffW0 + kBytesW0;
+constexpr std::uint32_t kOffW2 = kOffW1 + kBytesW1;
+constexpr std::uint32_t kOffW3 = kOffW2 + kBytesW1;
+constexpr std::uint32_t kOffA = kOffW3 + kBytesW3;
+constexpr std::uint32_t kOffBias = kOffA + kBytesA;
+constexpr std::uint32_t kOffBarrier = kOffBias + kBiases * 4;         // 8-byte aligned
+constexpr std::uint32_t kOffTmem = kOffBarrier + 8;
+constexpr std::size_t kTcSmem = kOffTmem + 8;
+static_assert(kOffBarrier % 8 == 0, "mbarrier alignment");
+static_assert(kTcSmem <= 227 * 1024, "shared memory");
+// An mbarrier wait gives up after this many polls and reports an error.
+constexpr std::uint32_t kWaitPolls = 1u << 26;
+
+// Byte offset of element (row, k) in a K-major no-swizzle operand of `rows` rows.
+__host__ __device__ constexpr std::uint32_t core_offset(std::uint32_t rows, std::uint32_t row, std::uint32_t k) {
+  return (k / 8) * (rows / 8) * 128 + (row / 8) * 128 + (row % 8) * 16 + (k % 8) * 2;
+}
+
+// Shared-memory matrix descriptor: start address, leading byte offset (K
+// blocks), stride byte offset (row groups), descriptor version 1, no swizzle.
+__device__ __forceinline__ std::uint64_t smem_descriptor(std::uint32_t address, std::uint32_t lbo,
+                                                         std::uint32_t sbo) {
+  std::uint64_t d = 0;
+  d |= std::uint64_t((address >> 4) & 0x3FFFu);
+  d |= std::uint64_t((lbo >> 4) & 0x3FFFu) << 16;
+  d |= std::uint64_t((sbo >> 4) & 0x3FFFu) << 32;
+  d |= std::uint64_t(1) << 46;
+  return d;
+}
+
+// Instruction descriptor of kind::f16: fp32 accumulator, bf16 A and B, both
+// K-major, M = 128, N = n.
+__host__ __device__ constexpr std::uint32_t instr_descriptor(std::uint32_t n) {
+  return (1u << 4) | (1u << 7) | (1u << 10) | ((n >> 3) << 17) | ((128u >> 4) << 24);
+}
+
+__device__ __forceinline__ void mma(std::uint32_t tmem, std::uint64_t a, std::uint64_t b, std::uint32_t idesc,
+                                    std::uint32_t accumulate) {
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t"
+      "}\n" ::"r"(tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+__device__ __forceinline__ void commit(std::uint32_t barrier) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(barrier)
+               : "memory");
+}
+
+__device__ __forceinline__ bool try_wait(std::uint32_t barrier, std::uint32_t phase) {
+  std::uint32_t done;
+  asm volatile(
+      "{\n\t"
+      ".reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t"
+      "}\n"
+      : "=r"(done)
+      : "r"(barrier), "r"(phase)
+      : "memory");
+  return done != 0;
+}
+
+__device__ __forceinline__ void fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void fence_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// 32 consecutive accumulator columns of this thread's TMEM lane.
+__device__ __forceinline__ void load32(std::uint32_t address, float (&v)[32]) {
+  std::uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+        "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+        "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(address));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.0f + erff(z * 0.70710678118654752f)); }
+
+__device__ __forceinline__ std::uint32_t pack(float lo, float hi) {
+  const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+  return *reinterpret_cast<const std::uint32_t*>(&v);
+}
+
+// Copies a row-major (rows x k) bf16 matrix from global memory into the
+// operand layout, zero rows from `valid` on.
+__device__ void stage_weights(unsigned char* smem, const std::uint16_t* w, std::uint32_t rows, std::uint32_t valid,
+                              std::uint32_t k) {
+  const std::uint32_t chunks = rows * (k / 8);
+  for (std::uint32_t c = threadIdx.x; c < chunks; c += blockDim.x) {
+    const std::uint32_t row = c / (k / 8), kb = c % (k / 8);
+    uint4 v = make_uint4(0u, 0u, 0u, 0u);
+    if (row < valid) v = *reinterpret_cast<const uint4*>(w + std::size_t(row) * k + kb * 8);
+    *reinterpret_cast<uint4*>(smem + core_offset(rows, row, kb * 8)) = v;
+  }
+}
+
+__global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_t* __restrict__ weights,
+                                                              const float* __restrict__ biases,
+                                                              const std::uint16_t* __restrict__ x, std::uint32_t n,
+                                                              float* __restrict__ y, std::uint32_t* error) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const std::uint32_t base = static_cast<std::uint32_t>(__cvta_generic_to_shared(smem));
+  const std::uint32_t barrier = base + kOffBarrier;
+  float* bias = reinterpret_cast<float*>(smem + kOffBias);
+  std::uint32_t* tmem_slot = reinterpret_cast<std::uint32_t*>(smem + kOffTmem);
+  __shared__ int ok;
+
+  stage_weights(smem + kOffW0, weights + kW0, kHidden, kHidden, kInput);
+  stage_weights(smem + kOffW1, weights + kW1, kHidden, kHidden, kHidden);
+  stage_weights(smem + kOffW2, weights + kW2, kHidden, kHidden, kHidden);
+  stage_weights(smem + kOffW3, weights + kW3, kOutputRows, kOutputPad, kHidden);
+  for (std::uint32_t i = threadIdx.x; i < kBiases; i += blockDim.x) bias[i] = biases[i];
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barrier), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    ok = 1;
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kOffTmem),
+                 "r"(kTmemColumns)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_async_smem();
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const std::uint32_t tmem = *tmem_slot;
+  const std::uint32_t warp = threadIdx.x >> 5;
+  const std::uint32_t lane_base = tmem + ((warp * 32u) << 16);
+  const std::uint32_t row = threadIdx.x;  // this thread's cell in a tile = its TMEM lane
+  std::uint32_t phase = 0;
+  unsigned char* a = smem + kOffA;
+
+  const std::uint32_t tiles = (n + kTile - 1) / kTile;
+  for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+    // The tile's features into the A operand (K = 96), zero rows past n.
+    const std::uint32_t cell = tile * kTile + row;
+#pragma unroll
+    for (std::uint32_t kb = 0; kb < kInput / 8; ++kb) {
+      uint4 v = make_uint4(0u, 0u, 0u, 0u);
+      if (cell < n) v = *reinterpret_cast<const uint4*>(x + std::size_t(cell) * kInput + kb * 8);
+      *reinterpret_cast<uint4*>(a + core_offset(kTile, row, kb * 8)) = v;
+    }
+    for (int layer = 0; layer < 4; ++layer) {
+      const std::uint32_t k = layer == 0 ? kInput : kHidden;
+      const std::uint32_t rows_b = layer == 3 ? kOutputRows : kHidden;
+      const std::uint32_t w_off = layer == 0 ? kOffW0 : (layer == 1 ? kOffW1 : (layer == 2 ? kOffW2 : kOffW3));
+      fence_async_smem();  // the operand rows written above, for the tensor cores
+      fence_before();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        fence_after();
+        const std::uint32_t idesc = instr_descriptor(rows_b);
+        for (std::uint32_t s = 0; s < k / 16; ++s) {
+          const std::uint64_t ad = smem_descriptor(base + kOffA + 2 * s * (kTile / 8) * 128, (kTile / 8) * 128, 128);
+          const std::uint64_t bd = smem_descriptor(base + w_off + 2 * s * (rows_b / 8) * 128, (rows_b / 8) * 128, 128);
+          mma(tmem, ad, bd, idesc, s > 0 ? 1u : 0u);
+        }
+        commit(barrier);
+        std::uint32_t polls = 0;
+        while (!try_wait(barrier, phase)) {
+          if (++polls > kWaitPolls) {
+            ok = 0;
+            if (error != nullptr) atomicExch(error, std::uint32_t(kStatusIterations));
+            break;
+          }
+        }
+      }
+      phase ^= 1u;
+      __syncthreads();
+      if (!ok) break;
+      fence_after();
+      if (layer < 3) {
+        const float* b = bias + (layer == 0 ? kB0 : (layer == 1 ? kB1 : kB2));
+#pragma unroll 1
+        for (std::uint32_t c = 0; c < kHidden / 32; ++c) {
+          float v[32];
+          load32(lane_base + c * 32, v);
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const std::uint32_t k0 = c * 32 + q * 8;
+            uint4 out;
+            out.x = pack(gelu(v[q * 8 + 0] + b[k0 + 0]), gelu(v[q * 8 + 1] + b[k0 + 1]));
+            out.y = pack(gelu(v[q * 8 + 2] + b[k0 + 2]), gelu(v[q * 8 + 3] + b[k0 + 3]));
+            out.z = pack(gelu(v[q * 8 + 4] + b[k0 + 4]), gelu(v[q * 8 + 5] + b[k0 + 5]));
+            out.w = pack(gelu(v[q * 8 + 6] + b[k0 + 6]), gelu(v[q * 8 + 7] + b[k0 + 7]));
+            *reinterpret_cast<uint4*>(a + core_offset(kTile, row, k0)) = out;
+          }
+        }
+      } else {
+        float v[32];
+        load32(lane_base, v);
+        if (cell < n) {
+#pragma unroll
+          for (int j = 0; j < kOutputs; ++j) y[std::size_t(cell) * kOutputs + j] = v[j] + bias[kB3 + j];
+        }
+      }
+    }
+    if (!ok) break;
+  }
+  fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns) : "memory");
+  }
+}
+
+}  // namespace
+
+int launch_forward_tc(const std::uint16_t* weights, const float* biases, const std::uint16_t* features,
+                      std::uint32_t n, float* outputs, std::uint32_t* error, cudaStream_t stream) {
+  if (n == 0) return 0;
+  cudaError_t e = cudaFuncSetAttribute(forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem));
+  if (e != cudaSuccess) return int(e);
+  int device = 0, sms = kSmCount;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  const std::uint32_t tiles = (n + kTile - 1) / kTile;
+  const std::uint32_t blocks = std::max(1u, std::min<std::uint32_t>(tiles, std::uint32_t(sms)));
+  forward_tc_kernel<<<blocks, kTile, kTcSmem, stream>>>(weights, biases, features, n, outputs, error);
+  count_launch();
+  return int(cudaGetLastError());
+}
+
+}  // namespace msb::mlp

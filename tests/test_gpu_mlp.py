@@ -67,6 +67,21 @@ def test_forward_matches_oracle(backend):
     assert np.array_equal(y7, y[:7])
 
 
+def test_tcgen05_inference_matches_the_training_forward(backend):
+    """The inference pass (tcgen05, TMEM accumulators) and the training
+    pass (mma.sync) compute the same network: equal up to the order of the
+    fp32 sums inside the tensor cores and the bf16 roundings that follow."""
+    net, p = network(4, backend._lib)
+    for n in (1, 127, 128, 129, 5000):
+        x = bf16_tensor(random_batch(n, 40 + n))
+        infer = net.forward(x).cpu().numpy()
+        train, _ = net.forward(x, keep=True)
+        train = train.cpu().numpy()
+        scale = max(np.abs(train).max(), 1e-6)
+        assert np.max(np.abs(infer - train)) <= 1e-2 * scale, (n, np.max(np.abs(infer - train)) / scale)
+        assert np.all(np.isfinite(infer))
+
+
 def test_backward_matches_oracle_gradient(backend):
     net, p = network(3, backend._lib)
     n = 777
