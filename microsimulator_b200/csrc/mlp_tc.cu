@@ -2,13 +2,14 @@
 // cores: tcgen05.mma with both operands in shared memory and the fp32
 // accumulator in tensor memory (TMEM).
 //
-// One CTA of 128 threads per SM works through 128-cell tiles.  Per layer:
+// One CTA of 512 threads per SM works through 128-cell tiles.  Per layer:
 // thread 0 issues the layer's K/16 MMAs (M = 128 cells, N = 128 outputs, or 16
-// for the output layer), commits them to an mbarrier, and every thread (one
-// TMEM lane = one cell) reads its row of the accumulator back with
-// tcgen05.ld, adds the bias, applies GELU, rounds to bf16 and writes the row
-// into the shared-memory operand of the next layer.  Weights stay in shared
-// memory for the whole launch.
+// for the output layer) and commits them to an mbarrier; then each of the 16
+// warps reads a 32-lane x 32-column block of the accumulator (warp w: lanes
+// of quarter w % 4, one per cell, columns 32 * (w / 4) on) with tcgen05.ld,
+// adds the bias, applies GELU, rounds to bf16 and writes it into the
+// shared-memory operand of the next layer.  Weights stay in shared memory for
+// the whole launch.
 //
 // Shared-memory operands use the canonical K-major layout without swizzle:
 // 8-row x 16-byte core matrices, rows of a core matrix 16 bytes apart, row
@@ -25,6 +26,7 @@ namespace msb::mlp {
 namespace {
 
 constexpr int kTile = 128;
+constexpr int kTcThreads = 512;
 constexpr std::uint32_t kTmemColumns = 128;
 constexpr std::uint32_t kOutputRows = 16;  // the output layer's N (8 weight rows, zero padded)
 // Bytes of each shared-memory operand.
@@ -139,7 +141,7 @@ __device__ void stage_weights(unsigned char* smem, const std::uint16_t* w, std::
   }
 }
 
-__global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_t* __restrict__ weights,
+__global__ void __launch_bounds__(kTcThreads, 1) forward_tc_kernel(const std::uint16_t* __restrict__ weights,
                                                               const float* __restrict__ biases,
                                                               const std::uint16_t* __restrict__ x, std::uint32_t n,
                                                               float* __restrict__ y, std::uint32_t* error) {
@@ -172,8 +174,9 @@ __global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_
   fence_after();
   const std::uint32_t tmem = *tmem_slot;
   const std::uint32_t warp = threadIdx.x >> 5;
-  const std::uint32_t lane_base = tmem + ((warp * 32u) << 16);
-  const std::uint32_t row = threadIdx.x;  // this thread's cell in a tile = its TMEM lane
+  const std::uint32_t quarter = warp % 4, chunk = warp / 4;
+  const std::uint32_t lane_base = tmem + ((quarter * 32u) << 16);
+  const std::uint32_t row = quarter * 32 + (threadIdx.x & 31);  // this thread's cell in a tile = its TMEM lane
   std::uint32_t phase = 0;
   unsigned char* a = smem + kOffA;
 
@@ -181,11 +184,12 @@ __global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_
   for (std::uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
     // The tile's features into the A operand (K = 96), zero rows past n.
     const std::uint32_t cell = tile * kTile + row;
-#pragma unroll
-    for (std::uint32_t kb = 0; kb < kInput / 8; ++kb) {
+    for (std::uint32_t e = threadIdx.x; e < std::uint32_t(kTile) * (kInput / 8); e += blockDim.x) {
+      const std::uint32_t r = e / (kInput / 8), kb = e % (kInput / 8);
+      const std::uint32_t c = tile * kTile + r;
       uint4 v = make_uint4(0u, 0u, 0u, 0u);
-      if (cell < n) v = *reinterpret_cast<const uint4*>(x + std::size_t(cell) * kInput + kb * 8);
-      *reinterpret_cast<uint4*>(a + core_offset(kTile, row, kb * 8)) = v;
+      if (c < n) v = *reinterpret_cast<const uint4*>(x + std::size_t(c) * kInput + kb * 8);
+      *reinterpret_cast<uint4*>(a + core_offset(kTile, r, kb * 8)) = v;
     }
     for (int layer = 0; layer < 4; ++layer) {
       const std::uint32_t k = layer == 0 ? kInput : kHidden;
@@ -218,8 +222,8 @@ __global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_
       fence_after();
       if (layer < 3) {
         const float* b = bias + (layer == 0 ? kB0 : (layer == 1 ? kB1 : kB2));
-#pragma unroll 1
-        for (std::uint32_t c = 0; c < kHidden / 32; ++c) {
+        {
+          const std::uint32_t c = chunk;
           float v[32];
           load32(lane_base + c * 32, v);
 #pragma unroll
@@ -233,7 +237,7 @@ __global__ void __launch_bounds__(kTile, 1) forward_tc_kernel(const std::uint16_
             *reinterpret_cast<uint4*>(a + core_offset(kTile, row, k0)) = out;
           }
         }
-      } else {
+      } else if (chunk == 0) {
         float v[32];
         load32(lane_base, v);
         if (cell < n) {
@@ -264,7 +268,7 @@ int launch_forward_tc(const std::uint16_t* weights, const float* biases, const s
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const std::uint32_t tiles = (n + kTile - 1) / kTile;
   const std::uint32_t blocks = std::max(1u, std::min<std::uint32_t>(tiles, std::uint32_t(sms)));
-  forward_tc_kernel<<<blocks, kTile, kTcSmem, stream>>>(weights, biases, features, n, outputs, error);
+  forward_tc_kernel<<<blocks, kTcThreads, kTcSmem, stream>>>(weights, biases, features, n, outputs, error);
   count_launch();
   return int(cudaGetLastError());
 }
