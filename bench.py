@@ -315,7 +315,8 @@ def sweep_arm(args, backend, local, rank, dist):
         cells.download(cat)
         sweep.split_into(cat, batch.worlds)
         for w in batch.worlds:
-            w.next_id = int(w.ids.max()) + 1
+            if len(w):
+                w.next_id = int(w.ids.max()) + 1
         return start.elapsed_time(end), report, colonies, len(cat)
 
     for k in range(max(args.warmup, 3)):

@@ -277,7 +277,11 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
 }
 
 template <int Threads, bool Lean>
+void allow_wide_clusters();
+
+template <int Threads, bool Lean>
 cudaError_t launch_shape(const BatchDesc& desc, int cluster, int clusters, cudaStream_t stream) {
+  if (cluster > 8) allow_wide_clusters<Threads, Lean>();
   cudaLaunchConfig_t config{};
   config.gridDim = dim3(unsigned(cluster * clusters));
   config.blockDim = dim3(Threads);
@@ -293,8 +297,16 @@ cudaError_t launch_shape(const BatchDesc& desc, int cluster, int clusters, cudaS
   return cudaLaunchKernelEx(&config, batch_solve_kernel<Threads, Lean>, desc);
 }
 
+// Clusters of 16 CTAs are beyond the portable size of 8 and must be allowed
+// per kernel first.
+template <int Threads, bool Lean>
+void allow_wide_clusters() {
+  cudaFuncSetAttribute(batch_solve_kernel<Threads, Lean>, cudaFuncAttributeNonPortableClusterSizeAllowed, 1);
+}
+
 template <int Threads, bool Lean>
 int resident_clusters(int cluster) {
+  if (cluster > 8) allow_wide_clusters<Threads, Lean>();
   cudaLaunchConfig_t config{};
   config.gridDim = dim3(unsigned(cluster));
   config.blockDim = dim3(Threads);

@@ -52,7 +52,7 @@ struct BatchDesc {
 
 // A launch shape of the batched solve: CTAs per cluster and threads per CTA.
 struct BatchShape {
-  int cluster;  // 1, 2, 4 or 8
+  int cluster;  // 1, 2, 4, 8 or 16 (16: a non-portable cluster size)
   int threads;  // 256 or 512
   bool lean;    // 64-register form (one gather in flight per thread, more resident warps)
 };

@@ -989,7 +989,7 @@ void tune_batch(Ctx& c, const msb::BatchDesc& d) {
   check(cudaEventCreate(&stop), "event");
   float best = -1.0f;
   for (const bool lean : {false, true}) for (const int threads : {256, 512}) {
-    for (const int cluster : {1, 2, 4, 8}) {
+    for (const int cluster : {1, 2, 4, 8, 16}) {
       const msb::BatchShape shape{cluster, threads, lean};
       const int resident = batch_resident_clusters(shape);
       if (resident <= 0) continue;

@@ -74,7 +74,8 @@ class ColonyBatch:
                                                                   dynamics)
         split_into(batch, self.worlds)
         for w in self.worlds:
-            w.next_id = int(w.ids.max()) + 1
+            if len(w):
+                w.next_id = int(w.ids.max()) + 1
         return report, colonies
 
     def divide(self, fraction: float, seed: int) -> None:

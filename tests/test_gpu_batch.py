@@ -56,7 +56,7 @@ def test_each_colony_steps_as_it_would_alone(backend):
         tuning = b.batch_tuning()
     finally:
         b.close()
-    assert tuning["cluster"] in (1, 2, 4, 8) and tuning["threads"] in (256, 512)
+    assert tuning["cluster"] in (1, 2, 4, 8, 16) and tuning["threads"] in (256, 512)
     assert tuning["box_scale"] >= 1.0
     assert np.array_equal(colonies["cells"], np.array(SIZES_after(worlds), dtype=np.uint32))
     same_plan = report.substeps == 1 and all(r.substeps == 1 for r in reports_alone)
@@ -160,3 +160,34 @@ def test_batch_rejects_what_it_cannot_step(backend):
             backend.advance_contact_dynamics_batch(cells, [len(cells)], [1.0], [1.0e4], DT, p)
     finally:
         backend.set_warm_start(0)
+
+
+def test_batch_with_empty_and_single_cell_colonies(backend):
+    """Empty colonies, a single cell and a colony of two touching cells step
+    together; the empty ones report nothing, the single cell grows freely."""
+    from microsimulator_b200.world import WorldState
+
+    w = settled_worlds()[3]  # 50 cells
+    empty = WorldState()
+    one = WorldState()
+    one.add_cell(position=(3.0, 4.0, 0.0), length=2.0, growth_rate=0.5)
+    pair = WorldState()
+    pair.add_cell(position=(-1.4, 0.0, 0.0), length=2.0)
+    pair.add_cell(position=(1.4, 0.0, 0.0), length=2.0)
+    worlds = [empty, w.copy(), one, empty.copy(), pair]
+    batch = sweep.ColonyBatch(worlds, [1.0] * 5, [1.0e4] * 5)
+    b = B200Backend(0)
+    try:
+        report, colonies = batch.step(b, DT, ContactDynamicsParameters(overlap_tolerance=TOLERANCE))
+    finally:
+        b.close()
+    assert list(colonies["cells"]) == [0, len(w), 1, 0, 2]
+    assert colonies["iterations"][0] == 0 and colonies["rows"][0] == 0
+    assert colonies["iterations"][3] == 0
+    assert np.all(colonies["status"] == 0)
+    grown = batch.worlds[2]
+    assert abs(float(grown.lengths[0]) - 2.02) < 1e-5
+    assert grown.position_x[0] == np.float32(3.0) and grown.position_y[0] == np.float32(4.0)
+    # The overlapping pair pushed apart symmetrically.
+    px = batch.worlds[4].position_x
+    assert px[0] < -1.4 and px[1] > 1.4 and abs(float(px[0] + px[1])) < 1e-4
