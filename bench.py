@@ -81,13 +81,13 @@ def divide(world, step, seed):
 
 class Clocks:
     """SM clock and throttle reasons sampled through NVML from a background
-    thread during a region (every 0.5 s, one device).  An external
+    thread during a region (every 50 ms, one device).  An external
     `nvidia-smi -lms` poller takes driver locks often enough to stall the
     step's host synchronizations, so the sampling stays in-process and light."""
 
     REASONS = {0x4: "sw_power_cap", 0x8: "hw_slowdown", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown"}
 
-    def __init__(self, device, period=0.5):
+    def __init__(self, device, period=0.05):
         self.device = device
         self.period = period
         self.samples = []

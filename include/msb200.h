@@ -458,6 +458,36 @@ int msb_mlp_adam(float* params, const float* grads, float* m, float* v, uint32_t
 int msb_set_warm_start_network(msb_context* context, const uint16_t* weights, const float* biases,
                                const float* scale);
 
+/* ---- Flow drift inside the stepper ----------------------------------------
+ *
+ * A fluid velocity field on a regular lattice of sites (the signal grid's
+ * SignalGridSpec shape/origin/spacing/obstacles with its
+ * SignalGridVelocityField, signals.hpp:116-156) that carries the cells:
+ * with ContactDynamicsParameters.flow_drift the stepper gives every body the
+ * drift of Simulation::flow_drift_rates (simulation.cpp:159-186) for each
+ * substep, an equivalent-spheroid Jeffery closure of the face velocities
+ * sampled with SignalGrid::sample_velocity (signals.cpp:923-955, clamped to
+ * the lattice, fluid sites only), and limits substeps so that no cell drifts
+ * more than a quarter of the smallest spacing (contact_dynamics.cpp:708-714).
+ * Face arrays: x_faces (shape_x + 1) * shape_y * shape_z, y_faces
+ * shape_x * (shape_y + 1) * shape_z, z_faces shape_x * shape_y * (shape_z + 1),
+ * x-major as signals.cpp:134-152; obstacles (optional) one byte per site,
+ * nonzero for solid. */
+typedef struct msb_flow_field {
+  uint32_t shape_x, shape_y, shape_z;
+  uint32_t reserved;
+  msb_vec3 origin;
+  msb_vec3 spacing;
+  const float* x_faces;
+  const float* y_faces;
+  const float* z_faces;
+  const uint8_t* obstacles;
+} msb_flow_field;
+
+/* Gives the context a flow field (copied from host memory) for steps with
+ * flow_drift = 1; a null field removes it (such steps then fail). */
+int msb_set_flow_field(msb_context* context, const msb_flow_field* field);
+
 /* ---- Batches of independent colonies (no counterpart in the reference) --
  *
  * One contact-dynamics step of many independent colonies at once, as a

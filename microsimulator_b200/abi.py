@@ -218,6 +218,21 @@ class ContactDynamicsOutputs(ctypes.Structure):
     ]
 
 
+class FlowField(ctypes.Structure):
+    _fields_ = [
+        ("shape_x", c_uint32),
+        ("shape_y", c_uint32),
+        ("shape_z", c_uint32),
+        ("reserved", c_uint32),
+        ("origin", Vec3),
+        ("spacing", Vec3),
+        ("x_faces", c_void_p),
+        ("y_faces", c_void_p),
+        ("z_faces", c_void_p),
+        ("obstacles", c_void_p),
+    ]
+
+
 class ColonyParameters(ctypes.Structure):
     _fields_ = [("drag", c_float), ("contact_stiffness", c_float)]
 
@@ -381,6 +396,7 @@ SIGNATURES = {
     "msb_launch_count": (c_uint64, [c_void_p]),
     "msb_last_step_phases": (c_int, [c_void_p, c_void_p, c_uint32]),
     "msb_set_warm_start": (c_int, [c_void_p, c_uint32]),
+    "msb_set_flow_field": (c_int, [c_void_p, c_void_p]),
     "msb_advance_contact_dynamics_batch": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_float, c_void_p,
                                                    c_void_p, c_void_p, c_void_p, c_void_p, c_int]),
     "msb_tune_batch": (c_int, [c_void_p]),

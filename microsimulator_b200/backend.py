@@ -277,6 +277,15 @@ class B200Backend:
             ctypes.byref(native_outputs) if native_outputs is not None else None, 1 if device else 0))
         return ContactDynamicsReport.from_native(report), reports
 
+    def set_flow_field(self, field) -> None:
+        """Gives the backend a flow field (a ``FlowField``) for steps with
+        ``flow_drift``; None removes it."""
+        if field is None:
+            self._check(self._lib.msb_set_flow_field(self._handle, None))
+            return
+        native = field.native()
+        self._check(self._lib.msb_set_flow_field(self._handle, ctypes.byref(native)))
+
     def tune_batch(self) -> None:
         """Ask for a new tuning of the batched launch at the next batch call."""
         self._check(self._lib.msb_tune_batch(self._handle))

@@ -29,6 +29,7 @@
 
 #include "../../include/msb200.h"
 #include "batch.h"
+#include "flow.h"
 #include "kernels.h"
 #include "solve.h"
 #include "step.h"
@@ -234,9 +235,6 @@ void validate_dynamics(const msb_contact_dynamics_parameters& p) {
     throw std::invalid_argument("contact growth fraction must be finite and positive");
   }
   if (p.max_iterations == 0) throw std::invalid_argument("contact dynamics iteration limit must be positive");
-  if (p.flow_drift != 0) {
-    throw std::invalid_argument("flow drift inside the contact solve is not supported by this backend");
-  }
   validate_growth(p.growth);
 }
 
@@ -472,6 +470,12 @@ struct msb_context {
   std::uint32_t guess_cells = 0;
   float guess_dt = 0.0f;
   bool has_drift = false;  // a loaded system with some non-zero drift
+  // The flow field of msb_set_flow_field, for steps with flow drift.
+  bool has_flow = false;
+  msb::FlowField flow{};
+  msb::DBuf<float> flow_x, flow_y, flow_z;
+  msb::DBuf<std::uint8_t> flow_obstacles;
+  float flow_travel_limit = 0.0f;
   msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
   msb::DBuf<std::uint32_t> inc_offsets;
   msb::DBuf<float4> inc_a, inc_b, resp_a, resp_b, accepted_a, accepted_b;
@@ -1218,7 +1222,7 @@ void guess_forces(Ctx& c, float dt, const msb_growth_load_response& growth) {
 Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, const msb_contact_parameters& cp,
                         const msb_constraint_contact_parameters& wp, bool probe, std::uint64_t& iterations) {
   const std::uint32_t n = c.n;
-  c.has_drift = false;  // the stepper's bodies carry no drift (flow drift is not supported)
+  c.has_drift = false;  // no drift unless flow drift writes it below
   if (c.colonies > 0) {
     // Every colony takes part in the substep's first search and test.
     check(cudaMemsetAsync(c.colony_active.p, 0xFF, c.colonies * 4ull, c.stream), "memset");
@@ -1230,6 +1234,13 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   mark(c, kPhaseRows);
   launch_make_bodies(n, c.state.view(), c.growth.p, c.fixed.p, c.initial.view(), p.drag,
                      {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p}, c.stream, colonies_of(c));
+  if (p.flow_drift != 0) {
+    // The flow's drift over this substep from its starting geometry
+    // (contact_dynamics.cpp:426-431).
+    launch_flow_drift(n, c.state.view(), c.fixed.p, c.flow, dt, {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p},
+                      c.scalars.p + kStatus, c.stream);
+    c.has_drift = true;
+  }
   mark(c, kPhaseSearch);
   const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches);
   mark(c, kPhaseRows);
@@ -1367,7 +1378,17 @@ StepOutcome advance(Ctx& c, float dt, const msb_contact_dynamics_parameters& p, 
   launch_growth_bound(n, c.state.view(), c.growth.p, dt, c.scalars.p + kGrowthBits, c.stream);
   read_scalars(c);
   const float growth = bits_to_float(c.host_scalars[kGrowthBits]);
-  const float pieces = std::max(1.0f, std::ceil(growth / p.max_growth_fraction));
+  float pieces = std::max(1.0f, std::ceil(growth / p.max_growth_fraction));
+  if (p.flow_drift != 0 && c.flow_travel_limit > 0.0f) {
+    // No cell drifts more than the travel limit in a substep
+    // (contact_dynamics.cpp:708-714).
+    reset_scalars(c);
+    launch_flow_speed(n, c.state.view(), c.fixed.p, c.flow, c.scalars.p + kGrowthBits, c.scalars.p + kStatus,
+                      c.stream);
+    read_scalars(c);
+    const float speed = bits_to_float(c.host_scalars[kGrowthBits]);
+    pieces = std::max(pieces, std::ceil(speed * dt / c.flow_travel_limit));
+  }
   if (!std::isfinite(pieces)) throw std::runtime_error("contact dynamics growth per step is not finite");
   const float longest = dt / pieces;
   const float shortest = std::ldexp(longest, -int(p.max_step_halvings));
@@ -1594,6 +1615,60 @@ int msb_last_step_solves(const msb_context* context, msb_solve_record* records, 
   *count = std::uint32_t(log.size());
   for (std::size_t k = 0; k < log.size() && k < capacity; ++k) records[k] = log[k];
   return log.size() > capacity ? MSB_ERR_CAPACITY : MSB_OK;
+}
+
+int msb_set_flow_field(msb_context* context, const msb_flow_field* field) {
+  if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  auto& c = *context;
+  return guarded(context, [&] {
+    c.has_flow = false;
+    if (field == nullptr) return;
+    const auto positive_finite = [](float v) { return std::isfinite(v) && v > 0.0f; };
+    if (field->shape_x == 0 || field->shape_y == 0 || field->shape_z == 0) {
+      throw std::invalid_argument("flow field shape must be positive");
+    }
+    if (!positive_finite(field->spacing.x) || !positive_finite(field->spacing.y) ||
+        !positive_finite(field->spacing.z)) {
+      throw std::invalid_argument("flow field spacing must be finite and positive");
+    }
+    if (!std::isfinite(field->origin.x) || !std::isfinite(field->origin.y) || !std::isfinite(field->origin.z)) {
+      throw std::invalid_argument("flow field origin must be finite");
+    }
+    if (field->x_faces == nullptr || field->y_faces == nullptr || field->z_faces == nullptr) {
+      throw std::invalid_argument("flow field faces must not be null");
+    }
+    const std::size_t sx = field->shape_x, sy = field->shape_y, sz = field->shape_z;
+    const std::size_t nx = (sx + 1) * sy * sz, ny = sx * (sy + 1) * sz, nz = sx * sy * (sz + 1);
+    const auto finite_all = [](const float* v, std::size_t count) {
+      for (std::size_t i = 0; i < count; ++i) {
+        if (!std::isfinite(v[i])) return false;
+      }
+      return true;
+    };
+    if (!finite_all(field->x_faces, nx) || !finite_all(field->y_faces, ny) || !finite_all(field->z_faces, nz)) {
+      throw std::invalid_argument("flow field velocities must be finite");
+    }
+    c.flow_x.ensure(nx);
+    c.flow_y.ensure(ny);
+    c.flow_z.ensure(nz);
+    check(cudaMemcpyAsync(c.flow_x.p, field->x_faces, nx * 4, cudaMemcpyHostToDevice, c.stream), "copy flow");
+    check(cudaMemcpyAsync(c.flow_y.p, field->y_faces, ny * 4, cudaMemcpyHostToDevice, c.stream), "copy flow");
+    check(cudaMemcpyAsync(c.flow_z.p, field->z_faces, nz * 4, cudaMemcpyHostToDevice, c.stream), "copy flow");
+    const std::uint8_t* obstacles = nullptr;
+    if (field->obstacles != nullptr) {
+      c.flow_obstacles.ensure(sx * sy * sz);
+      check(cudaMemcpyAsync(c.flow_obstacles.p, field->obstacles, sx * sy * sz, cudaMemcpyHostToDevice, c.stream),
+            "copy flow");
+      obstacles = c.flow_obstacles.p;
+    }
+    sync(c);
+    c.flow = {field->shape_x, field->shape_y, field->shape_z,
+              make_float3(field->origin.x, field->origin.y, field->origin.z),
+              make_float3(field->spacing.x, field->spacing.y, field->spacing.z),
+              c.flow_x.p, c.flow_y.p, c.flow_z.p, obstacles};
+    c.flow_travel_limit = 0.25f * std::min({field->spacing.x, field->spacing.y, field->spacing.z});
+    c.has_flow = true;
+  });
 }
 
 int msb_set_warm_start(msb_context* context, uint32_t mode) {
@@ -1926,6 +2001,9 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     load_cells(c, *cells, device_pointers);
     load_constraints(c, constraints, constraint_count);
     c.has_memory = c.has_memory && (c.warm_start_mode & kWarmCarry) != 0;
+    if (dynamics->flow_drift != 0 && !c.has_flow) {
+      throw std::invalid_argument("flow drift requires a flow field (msb_set_flow_field)");
+    }
     if (c.has_guess && c.guess_cells != c.n) {
       c.has_guess = false;
       throw std::invalid_argument("the motion guess covers " + std::to_string(c.guess_cells) +
@@ -1986,6 +2064,7 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     if ((c.warm_start_mode & ~kWarmCarry) != 0) {
       throw std::invalid_argument("a batch takes no motion guess or warm-start network");
     }
+    if (dynamics->flow_drift != 0) throw std::invalid_argument("a batch takes no flow drift");
     std::vector<std::uint32_t> offsets(colony_count + 1, 0);
     std::vector<float> drag(colony_count), stiffness(colony_count), tolerance(colony_count), solve_tol(colony_count);
     for (std::uint32_t i = 0; i < colony_count; ++i) {

@@ -192,3 +192,41 @@ def empty_bodies(count: int) -> np.ndarray:
     bodies = np.zeros(count, dtype=abi.CONTACT_BODY_DTYPE)
     bodies["axis"][:, 0] = 1.0
     return bodies
+
+
+@dataclass
+class FlowField:
+    """A fluid velocity field on a lattice of sites, as the reference's
+    SignalGridSpec (shape, origin, spacing, obstacles) with its
+    SignalGridVelocityField: face velocities x-major,
+    x_faces (sx + 1, sy, sz), y_faces (sx, sy + 1, sz), z_faces (sx, sy, sz + 1),
+    obstacles (sx, sy, sz) nonzero for solid sites."""
+
+    shape: tuple
+    origin: tuple
+    spacing: tuple
+    x_faces: np.ndarray
+    y_faces: np.ndarray
+    z_faces: np.ndarray
+    obstacles: np.ndarray | None = None
+
+    def arrays(self):
+        sx, sy, sz = self.shape
+        xf = np.ascontiguousarray(self.x_faces, dtype=np.float32).reshape(-1)
+        yf = np.ascontiguousarray(self.y_faces, dtype=np.float32).reshape(-1)
+        zf = np.ascontiguousarray(self.z_faces, dtype=np.float32).reshape(-1)
+        if xf.size != (sx + 1) * sy * sz or yf.size != sx * (sy + 1) * sz or zf.size != sx * sy * (sz + 1):
+            raise ValueError("flow face arrays do not match the shape")
+        ob = None
+        if self.obstacles is not None:
+            ob = np.ascontiguousarray(self.obstacles, dtype=np.uint8).reshape(-1)
+            if ob.size != sx * sy * sz:
+                raise ValueError("flow obstacles do not match the shape")
+        return xf, yf, zf, ob
+
+    def native(self) -> abi.FlowField:
+        xf, yf, zf, ob = self.arrays()
+        self._keep = (xf, yf, zf, ob)
+        return abi.FlowField(self.shape[0], self.shape[1], self.shape[2], 0, abi.Vec3(*self.origin),
+                             abi.Vec3(*self.spacing), abi.ptr(xf), abi.ptr(yf), abi.ptr(zf),
+                             abi.ptr(ob) if ob is not None else None)

@@ -365,6 +365,19 @@ class Reference(_Checker):
         return _advance(self, "advance_contact_dynamics", (), world, constraints, dt, dynamics,
                         contacts, constraint_parameters)
 
+    def flow_step(self, world, field, dt, dynamics=None) -> ContactDynamicsReport:
+        """One Simulation::step of the reference with flow drift in `field`
+        (a microsimulator_b200.types.FlowField); `world` (ids 1..n in slot
+        order) is updated in place."""
+        dynamics = dynamics or ContactDynamicsParameters()
+        cells = world.arrays()
+        native = field.native()
+        dyn = dynamics.native()
+        report = abi.ContactDynamicsReport()
+        self._call("flow_step", ctypes.byref(cells), ctypes.byref(native), c_float(dt), ctypes.byref(dyn),
+                   ctypes.byref(report))
+        return ContactDynamicsReport.from_native(report)
+
     # -- a world held across calls (bench) ------------------------------
     def world_create(self, world, constraints=None):
         cells = world.arrays()

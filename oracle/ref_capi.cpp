@@ -16,6 +16,8 @@
 //   contact_system_diagonal_bound             cpp/cpu/cpu_contact_dynamics.cpp:247-260
 //   detail::advance_contact_dynamics          cpp/core/contact_dynamics.cpp:676-782
 //   WorldState::divide                        cpp/core/world_state.cpp:238-276
+//   Simulation::step with flow drift          cpp/core/simulation.cpp:387-488 (a Simulation
+//                                             with a signal grid and velocity field)
 
 #include <algorithm>
 #include <cstring>
@@ -31,6 +33,8 @@
 #include "microsimulator/constraints.hpp"
 #include "microsimulator/contact_dynamics.hpp"
 #include "microsimulator/contact_graph.hpp"
+#include "microsimulator/signals.hpp"
+#include "microsimulator/simulation.hpp"
 #include "microsimulator/threads.hpp"
 #include "microsimulator/world_state.hpp"
 
@@ -417,6 +421,69 @@ int ref_advance_contact_dynamics(msb_cell_arrays* cells, const msb_constraint* c
         }
       }
     }
+  });
+}
+
+// One Simulation::step(dt, dynamics) of the reference on the given cells
+// (ids 1..n in slot order, as Simulation::add_cell assigns them) with a
+// signal grid that holds the given velocity field: the flow-drift path.
+int ref_flow_step(msb_cell_arrays* cells, const msb_flow_field* field, float dt,
+                  const msb_contact_dynamics_parameters* dynamics, msb_contact_dynamics_report* report) {
+  return guarded([&] {
+    ms::Simulation sim(ms::BackendKind::cpu);
+    // The signal grid first: Simulation wants its geometry before cells.
+    ms::SignalGridSpec spec;
+    // One inert signal: the reference's signal grid needs at least one, and
+    // with zero diffusion and advection it leaves the mechanics untouched.
+    spec.signal_count = 1;
+    spec.diffusion = {0.0F};
+    spec.advection = {ms::Vec3{}};
+    // Implicit, so that a fast test flow meets no explicit stability bound.
+    spec.integration = ms::SignalIntegrationKind::backward_euler;
+    spec.shape = {field->shape_x, field->shape_y, field->shape_z};
+    spec.origin = {field->origin.x, field->origin.y, field->origin.z};
+    spec.spacing = {field->spacing.x, field->spacing.y, field->spacing.z};
+    const std::size_t sites = std::size_t(field->shape_x) * field->shape_y * field->shape_z;
+    if (field->obstacles != nullptr) spec.obstacles.assign(field->obstacles, field->obstacles + sites);
+    ms::SignalGridVelocityField velocity;
+    velocity.x_faces.assign(field->x_faces, field->x_faces + std::size_t(field->shape_x + 1) * field->shape_y *
+                                                                 field->shape_z);
+    velocity.y_faces.assign(field->y_faces, field->y_faces + std::size_t(field->shape_x) * (field->shape_y + 1) *
+                                                                 field->shape_z);
+    velocity.z_faces.assign(field->z_faces, field->z_faces + std::size_t(field->shape_x) * field->shape_y *
+                                                                 (field->shape_z + 1));
+    spec.velocity_field = velocity;
+    sim.configure_signal_grid(spec);
+    for (std::size_t s = 0; s < cells->count; ++s) {
+      ms::CellInit init;
+      init.position = {cells->position_x[s], cells->position_y[s], cells->position_z[s]};
+      init.direction = {cells->direction_x[s], cells->direction_y[s], cells->direction_z[s]};
+      init.length = cells->lengths[s];
+      init.radius = cells->radii[s];
+      init.growth_rate = cells->growth_rates != nullptr ? cells->growth_rates[s] : 0.0F;
+      init.fixed = cells->fixed != nullptr && cells->fixed[s] != 0;
+      sim.add_cell(init);
+    }
+    auto p = dynamics_parameters(*dynamics);
+    p.flow_drift = true;
+    const auto result = sim.step(dt, p);
+    for (const auto& cell : sim.cells()) {
+      const std::size_t s = cell.slot;
+      if (s >= cells->count) continue;
+      cells->position_x[s] = cell.position.x;
+      cells->position_y[s] = cell.position.y;
+      cells->position_z[s] = cell.position.z;
+      cells->direction_x[s] = cell.direction.x;
+      cells->direction_y[s] = cell.direction.y;
+      cells->direction_z[s] = cell.direction.z;
+      cells->lengths[s] = cell.length;
+    }
+    report->substeps = result.report.substeps;
+    report->halvings = result.report.halvings;
+    report->refinements = result.report.refinements;
+    report->iterations = result.report.iterations;
+    report->max_rows = result.report.max_rows;
+    report->max_overlap = result.report.max_overlap;
   });
 }
 

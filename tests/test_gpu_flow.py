@@ -1,0 +1,126 @@
+"""Flow drift inside the stepper (msb_set_flow_field + flow_drift) against
+the reference's own Simulation::step with a signal grid that holds the same
+velocity field: the Jeffery-closure drift of every body, obstacles, and the
+travel limit on substeps."""
+
+import numpy as np
+import pytest
+
+from microsimulator_b200 import workloads
+from microsimulator_b200.backend import B200Backend
+from microsimulator_b200.types import ContactDynamicsParameters, FlowField
+from microsimulator_b200.world import WorldState
+
+pytestmark = pytest.mark.gpu
+
+DT = 0.02
+
+
+def field(shape=(24, 20, 1), spacing=(2.0, 2.0, 1.0), origin=(-4.0, -4.0, -0.5), strength=1.0, solid=True, seed=0):
+    """A swirling shear flow sampled on the faces of the lattice, with a few
+    solid sites."""
+    sx, sy, sz = shape
+    ox, oy, oz = origin
+    hx, hy, hz = spacing
+    rng = np.random.default_rng(seed)
+    xf = np.zeros((sx + 1, sy, sz), np.float32)
+    yf = np.zeros((sx, sy + 1, sz), np.float32)
+    zf = np.zeros((sx, sy, sz + 1), np.float32)
+    for i in range(sx + 1):
+        for j in range(sy):
+            x, y = ox + i * hx, oy + (j + 0.5) * hy
+            xf[i, j, :] = strength * (0.3 * y - 0.05 * x + 0.02 * rng.standard_normal())
+    for i in range(sx):
+        for j in range(sy + 1):
+            x, y = ox + (i + 0.5) * hx, oy + j * hy
+            yf[i, j, :] = strength * (-0.2 * x + 0.05 * y + 0.02 * rng.standard_normal())
+    # Closed faces carry no flow: the lattice's boundary, and every face of a
+    # solid site (the reference's signal grid rejects a field otherwise).
+    xf[0], xf[sx] = 0.0, 0.0
+    yf[:, 0], yf[:, sy] = 0.0, 0.0
+    obstacles = None
+    if solid:
+        obstacles = np.zeros((sx, sy, sz), np.uint8)
+        obstacles[3:5, 12:14, :] = 1
+        obstacles[15, 4, :] = 1
+        for i, j, _ in np.argwhere(obstacles):
+            xf[i, j], xf[i + 1, j] = 0.0, 0.0
+            yf[i, j], yf[i, j + 1] = 0.0, 0.0
+    return FlowField(shape, origin, spacing, xf, yf, zf, obstacles)
+
+
+def colony(n=150, seed=5):
+    w = workloads.colony_1k(seed=seed, n=n, side=30.0, growth_rate=0.5)
+    fresh = WorldState.from_arrays(np.stack([w.position_x, w.position_y, w.position_z], 1),
+                                   np.stack([w.direction_x, w.direction_y, w.direction_z], 1), w.lengths, 0.5,
+                                   growth_rates=0.5)
+    return fresh
+
+
+def test_drift_of_isolated_cells_is_the_references(backend, reference):
+    world = WorldState()
+    world.add_cell(position=(1.0, 2.0, 0.0), direction=(0.6, 0.8, 0.0), length=2.5, growth_rate=0.0)
+    world.add_cell(position=(20.0, 10.0, 0.0), direction=(1.0, 0.0, 0.0), length=3.0, growth_rate=0.0)
+    world.add_cell(position=(7.0, 21.0, 0.0), direction=(0.0, 1.0, 0.0), length=2.0, growth_rate=0.0)
+    f = field()
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        rg = backend.advance_contact_dynamics(gpu, None, DT, p)
+    finally:
+        backend.set_flow_field(None)
+    rr = reference.flow_step(ref, f, DT, p)
+    assert rg.report.substeps == rr.substeps
+    moved = np.max(np.abs(gpu.geometry()[:, :3] - world.geometry()[:, :3]))
+    assert moved > 1e-3  # the flow carried them
+    # No contacts: the step is the drift alone, the same float operations.
+    assert np.array_equal(gpu.geometry(), ref.geometry()), np.max(np.abs(gpu.geometry() - ref.geometry()))
+
+
+@pytest.mark.parametrize("solid", [False, True])
+def test_colony_in_flow_matches_reference(backend, reference, solid):
+    world = colony()
+    f = field(solid=solid, seed=3)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        rg = backend.advance_contact_dynamics(gpu, None, DT, p)
+    finally:
+        backend.set_flow_field(None)
+    rr = reference.flow_step(ref, f, DT, p)
+    assert rg.report.substeps == rr.substeps
+    spread = np.max(np.abs(gpu.geometry()[:, :3] - ref.geometry()[:, :3]))
+    assert spread < 4 * 5e-4, spread
+
+
+def test_travel_limit_splits_the_step_as_the_reference(backend, reference):
+    world = colony(n=60, seed=7)
+    f = field(strength=40.0, solid=False, seed=4)  # drift far beyond a quarter spacing per step
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        rg = backend.advance_contact_dynamics(gpu, None, DT, p)
+    finally:
+        backend.set_flow_field(None)
+    rr = reference.flow_step(ref, f, DT, p)
+    assert rr.substeps > 1
+    assert rg.report.substeps == rr.substeps
+    spread = np.max(np.abs(gpu.geometry()[:, :3] - ref.geometry()[:, :3]))
+    assert spread < 4 * 5e-4, spread
+
+
+def test_flow_drift_needs_a_field(backend):
+    world = colony(n=20)
+    p = ContactDynamicsParameters(flow_drift=True)
+    before = world.copy()
+    with pytest.raises(ValueError):
+        backend.advance_contact_dynamics(world, None, DT, p)
+    assert np.array_equal(before.geometry(), world.geometry())
+    with pytest.raises(ValueError):
+        bad = field()
+        bad.x_faces = bad.x_faces.copy()
+        bad.x_faces[0, 0, 0] = np.nan
+        backend.set_flow_field(bad)
