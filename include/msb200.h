@@ -283,6 +283,50 @@ int msb_find_external_contacts(msb_context* context, const msb_cell_arrays* cell
                                uint32_t every_face, msb_external_contact* contacts,
                                uint64_t capacity, uint64_t* count);
 
+/* ----------------------------------------------------- contact graph index */
+
+/* The index arrays of a ContactGraph (contact_graph.hpp:40-63): per slot the
+ * indices of its contacts in contact order (incident_contact_indices,
+ * contact_graph.cpp:376-384) and its distinct partner ids in ascending order
+ * (neighbor_ids, contact_graph.cpp:386-394), each as cell_count + 1 offsets
+ * into one packed array, as the constructor lays them out
+ * (contact_graph.cpp:302-349).  All arrays are host or device memory as the
+ * call's device_pointers says. */
+typedef struct msb_contact_graph_index {
+  uint64_t* incidence_offsets;  /* cell_count + 1 */
+  uint64_t* incidence_contacts; /* 2 * contact count */
+  uint64_t* neighbor_offsets;   /* cell_count + 1; null with neighbor_ids: no neighbour index */
+  uint64_t* neighbor_ids;       /* neighbor_capacity ids; 2 * contact count always suffices */
+  uint64_t neighbor_capacity;
+  uint64_t neighbor_count;      /* out: the packed neighbour ids' count */
+} msb_contact_graph_index;
+
+/* ContactGraph(cell_count, contacts) (contact_graph.cpp:302-349) for a
+ * caller's contact list: validates every contact as the constructor does
+ * (contact_graph.cpp:217-237; the lowest failing contact's reason is the
+ * error text, MSB_ERR_INVALID_ARGUMENT) and builds the index on the device.
+ * MSB_ERR_OVERFLOW beyond the slot index space (cell_count >= 2^32 - 1) or
+ * 2^31 - 1 contacts; MSB_ERR_CAPACITY (neighbor_count set) when the
+ * neighbour ids do not fit. */
+int msb_build_contact_graph(msb_context* context, const msb_cell_contact* contacts, uint64_t count,
+                            uint64_t cell_count, uint32_t device_pointers, msb_contact_graph_index* index);
+
+/* ExternalContactGraph(cell_count, contacts) (cpp/core/constraints.cpp:288-307):
+ * validation (constraints.cpp:126-145) and the per-slot incidence
+ * (incident_contact_indices): cell_count + 1 offsets and `count` indices. */
+int msb_build_external_contact_graph(msb_context* context, const msb_external_contact* contacts, uint64_t count,
+                                     uint64_t cell_count, uint32_t device_pointers, uint64_t* incidence_offsets,
+                                     uint64_t* incidence_contacts);
+
+/* ComputeBackend::find_cell_contacts returning its whole ContactGraph
+ * (backend.hpp:35-36, cpu_contacts.cpp:211): the contacts of
+ * msb_find_cell_contacts and, from the same device-resident list, the index
+ * of msb_build_contact_graph (host arrays; cell_count = cells->count).
+ * `index` may be null (contacts only). */
+int msb_find_cell_contact_graph(msb_context* context, const msb_cell_arrays* cells,
+                                const msb_contact_parameters* parameters, msb_cell_contact* contacts,
+                                uint64_t capacity, uint64_t* count, msb_contact_graph_index* index);
+
 /* --------------------------------------------------------- contact solve */
 
 /* ComputeBackend::solve_contact_forces (backend.hpp:41-43): Barzilai-Borwein

@@ -233,6 +233,17 @@ class FlowField(ctypes.Structure):
     ]
 
 
+class ContactGraphIndex(ctypes.Structure):
+    _fields_ = [
+        ("incidence_offsets", c_void_p),
+        ("incidence_contacts", c_void_p),
+        ("neighbor_offsets", c_void_p),
+        ("neighbor_ids", c_void_p),
+        ("neighbor_capacity", c_uint64),
+        ("neighbor_count", c_uint64),
+    ]
+
+
 class ColonyParameters(ctypes.Structure):
     _fields_ = [("drag", c_float), ("contact_stiffness", c_float)]
 
@@ -332,6 +343,14 @@ SIGNATURES = {
         c_int,
         [c_void_p, POINTER(CellArrays), POINTER(ContactParameters), c_void_p, c_uint64, POINTER(c_uint64)],
     ),
+    "msb_find_cell_contact_graph": (
+        c_int,
+        [c_void_p, POINTER(CellArrays), POINTER(ContactParameters), c_void_p, c_uint64, POINTER(c_uint64),
+         c_void_p],
+    ),
+    "msb_build_contact_graph": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_void_p]),
+    "msb_build_external_contact_graph": (
+        c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_void_p, c_void_p]),
     "msb_find_external_contacts": (
         c_int,
         [

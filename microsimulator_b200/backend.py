@@ -16,6 +16,7 @@ from ctypes import c_float, c_uint32, c_uint64, c_void_p
 import numpy as np
 
 from . import abi
+from .graph import ContactGraph, ExternalContactGraph
 from .types import (
     ConstraintContactParameters,
     ContactDynamicsParameters,
@@ -161,6 +162,69 @@ class B200Backend:
             abi.CELL_CONTACT_DTYPE,
             8 * len(world),
         )
+
+    def find_cell_contact_graph(self, world, parameters: ContactParameters | None = None) -> ContactGraph:
+        """find_cell_contacts returning the whole ContactGraph: the contacts
+        and their incidence and neighbour index, built on the device from the
+        contacts as found."""
+        parameters = parameters or ContactParameters()
+        cells = world.arrays()
+        native = parameters.native()
+        n = len(world)
+        capacity = max(self._capacity, 8 * n)
+        while True:
+            contacts = np.zeros(capacity, dtype=abi.CELL_CONTACT_DTYPE)
+            index, arrays = self._index_arrays(n, 2 * capacity, True)
+            count = c_uint64(0)
+            status = self._lib.msb_find_cell_contact_graph(self._handle, ctypes.byref(cells), ctypes.byref(native),
+                                                           c_void_p(abi.ptr(contacts)), capacity,
+                                                           ctypes.byref(count), ctypes.byref(index))
+            if status == abi.ERR_CAPACITY and count.value > capacity:
+                capacity = int(count.value) + 16
+                continue
+            self._check(status)
+            self._capacity = max(self._capacity, int(count.value))
+            return self._graph(n, contacts[: count.value].copy(), index, arrays)
+
+    def build_contact_graph(self, contacts: np.ndarray, cell_count: int) -> ContactGraph:
+        """ContactGraph(cell_count, contacts) (contact_graph.cpp:302-349) on
+        the device: validation, incidence and neighbours."""
+        records = np.ascontiguousarray(contacts, dtype=abi.CELL_CONTACT_DTYPE)
+        index, arrays = self._index_arrays(cell_count, 2 * len(records), True)
+        self._check(self._lib.msb_build_contact_graph(self._handle, c_void_p(abi.ptr(records)), len(records),
+                                                      cell_count, 0, ctypes.byref(index)))
+        return self._graph(cell_count, records.copy(), index, arrays)
+
+    def build_external_contact_graph(self, contacts: np.ndarray, cell_count: int) -> ExternalContactGraph:
+        """ExternalContactGraph(cell_count, contacts) (constraints.cpp:288-307)."""
+        records = np.ascontiguousarray(contacts, dtype=abi.EXTERNAL_CONTACT_DTYPE)
+        offsets = np.zeros(int(cell_count) + 1, dtype=np.uint64)
+        indices = np.zeros(max(1, len(records)), dtype=np.uint64)
+        self._check(self._lib.msb_build_external_contact_graph(
+            self._handle, c_void_p(abi.ptr(records)), len(records), cell_count, 0, c_void_p(abi.ptr(offsets)),
+            c_void_p(abi.ptr(indices))))
+        return ExternalContactGraph(cell_count, records.copy(), offsets, indices[: len(records)])
+
+    @staticmethod
+    def _index_arrays(cell_count: int, entries: int, neighbors: bool):
+        arrays = {
+            "incidence_offsets": np.zeros(int(cell_count) + 1, dtype=np.uint64),
+            "incidence_contacts": np.zeros(max(1, entries), dtype=np.uint64),
+        }
+        if neighbors:
+            arrays["neighbor_offsets"] = np.zeros(int(cell_count) + 1, dtype=np.uint64)
+            arrays["neighbor_ids"] = np.zeros(max(1, entries), dtype=np.uint64)
+        index = abi.ContactGraphIndex()
+        for name, array in arrays.items():
+            setattr(index, name, abi.ptr(array))
+        index.neighbor_capacity = entries if neighbors else 0
+        return index, arrays
+
+    @staticmethod
+    def _graph(cell_count, contacts, index, arrays) -> ContactGraph:
+        return ContactGraph(cell_count, contacts, arrays["incidence_offsets"],
+                            arrays["incidence_contacts"][: 2 * len(contacts)], arrays["neighbor_offsets"],
+                            arrays["neighbor_ids"][: index.neighbor_count])
 
     def find_external_contacts(self, world, constraints, parameters: ConstraintContactParameters | None = None,
                                every_face: bool = False) -> np.ndarray:

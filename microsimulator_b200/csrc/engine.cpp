@@ -30,6 +30,7 @@
 #include "../../include/msb200.h"
 #include "batch.h"
 #include "flow.h"
+#include "graph.h"
 #include "kernels.h"
 #include "solve.h"
 #include "step.h"
@@ -527,6 +528,13 @@ struct msb_context {
   // outputs staging for host calls
   msb::DBuf<float> out_velocities, out_loads, out_increments;
   msb::DBuf<std::uint8_t> records;
+
+  // contact graph index: a copy of host contacts, scratch, staging of the
+  // index for host calls, and the validation words
+  msb::DBuf<std::uint8_t> graph_contacts;
+  msb::DBuf<std::uint32_t> graph_scratch;
+  msb::DBuf<std::uint64_t> graph_incidence_offsets, graph_incidence, graph_neighbor_offsets, graph_neighbors;
+  msb::DBuf<unsigned long long> graph_words;
 };
 
 namespace msb {
@@ -1537,6 +1545,113 @@ int guarded(msb_context* c, Body&& body) {
   }
 }
 
+// ---- contact graph index (graph.cu)
+
+// The reference's validate_contact texts, by the reason codes of graph.cu.
+constexpr const char* kCellContactReasons[] = {
+    "contact is valid",
+    "contact cell identifiers are not canonical",
+    "contact slots are invalid",
+    "cell contact ordinal exceeds the capsule-pair contract",
+    "contact contains a non-finite or invalid field",
+    "contact normal is not unit length",
+};
+constexpr const char* kExternalContactReasons[] = {
+    "external contact is valid",
+    "external contact has an invalid identity",
+    "external contact cell slot is invalid",
+    "external contact contains an invalid tag",
+    "external contact contains a non-finite or invalid field",
+    "external contact normal is not unit length",
+};
+
+// Index arrays in device memory.
+struct GraphArrays {
+  std::uint64_t* incidence_offsets;
+  std::uint64_t* incidence;
+  std::uint64_t* neighbor_offsets;  // null: no neighbour index
+  std::uint64_t* neighbors;
+  std::uint64_t neighbor_capacity;
+};
+
+void check_graph_size(std::uint64_t cell_count, std::uint64_t count, bool external) {
+  // checked_offset_count (contact_graph.cpp:209-215)
+  if (cell_count > 0xFFFFFFFFull) throw std::overflow_error("contact graph exceeds the slot index space");
+  if ((external ? count : 2 * count) >= 0xFFFFFFFFull) {
+    throw std::overflow_error("contact incidence exceeds the 32-bit entry index space");
+  }
+}
+
+// Validates `count` device-resident contacts and builds their index into
+// `out`; returns the packed neighbour count (0 without a neighbour index).
+std::uint64_t build_graph(Ctx& c, const void* contacts, std::uint64_t count, std::uint64_t cell_count,
+                          bool external, const GraphArrays& out) {
+  check_graph_size(cell_count, count, external);
+  c.graph_words.ensure(4);
+  launch_validate_contacts(contacts, count, cell_count, external, c.graph_words.p, c.stream);
+  unsigned long long words[2] = {0, 0};
+  check(cudaMemcpyAsync(words, c.graph_words.p, sizeof(words), cudaMemcpyDeviceToHost, c.stream), "copy words");
+  sync(c);
+  if (words[0] != ~0ull) {
+    const unsigned reason = std::min(unsigned(words[0] & 0xFFu), 5u);
+    throw std::invalid_argument(external ? kExternalContactReasons[reason] : kCellContactReasons[reason]);
+  }
+  const std::uint64_t entries = external ? count : 2 * count;
+  c.graph_scratch.ensure(graph_scratch_words(entries));
+  build_incidence(contacts, count, cell_count, external, out.incidence_offsets, out.incidence, c.graph_scratch.p,
+                  c.stream);
+  if (external || out.neighbor_offsets == nullptr) return 0;
+  build_neighbors(contacts, count, cell_count, words[1], out.incidence_offsets, out.neighbor_offsets, out.neighbors,
+                  out.neighbor_capacity, c.graph_scratch.p, c.graph_words.p + 2, c.stream);
+  unsigned long long total = 0;
+  check(cudaMemcpyAsync(&total, c.graph_words.p + 2, sizeof(total), cudaMemcpyDeviceToHost, c.stream),
+        "copy count");
+  sync(c);
+  return total;
+}
+
+// Device staging for an index the caller wants in host memory.
+GraphArrays graph_staging(Ctx& c, std::uint64_t cell_count, std::uint64_t entries, bool neighbors) {
+  GraphArrays g{};
+  g.incidence_offsets = c.graph_incidence_offsets.ensure(cell_count + 1);
+  g.incidence = c.graph_incidence.ensure(std::max<std::uint64_t>(entries, 1));
+  if (neighbors) {
+    g.neighbor_offsets = c.graph_neighbor_offsets.ensure(cell_count + 1);
+    g.neighbors = c.graph_neighbors.ensure(std::max<std::uint64_t>(entries, 1));
+    g.neighbor_capacity = entries;  // distinct partners never outnumber entries
+  }
+  return g;
+}
+
+void copy_out(Ctx& c, void* host, const void* device, std::uint64_t bytes) {
+  if (bytes == 0) return;
+  check(cudaMemcpyAsync(host, device, bytes, cudaMemcpyDeviceToHost, c.stream), "copy index");
+}
+
+// Copies a staged index to the caller's host arrays (`index` names them).
+void copy_graph_out(Ctx& c, const GraphArrays& g, std::uint64_t cell_count, std::uint64_t entries,
+                    std::uint64_t neighbors, msb_contact_graph_index& index) {
+  copy_out(c, index.incidence_offsets, g.incidence_offsets, (cell_count + 1) * 8);
+  copy_out(c, index.incidence_contacts, g.incidence, entries * 8);
+  if (g.neighbor_offsets != nullptr) {
+    copy_out(c, index.neighbor_offsets, g.neighbor_offsets, (cell_count + 1) * 8);
+    copy_out(c, index.neighbor_ids, g.neighbors, neighbors * 8);
+  }
+  sync(c);
+}
+
+// The checks on a caller's index record shared by the graph calls.
+bool check_index(const msb_contact_graph_index& index, std::uint64_t count) {
+  if (index.incidence_offsets == nullptr || (count > 0 && index.incidence_contacts == nullptr)) {
+    throw std::invalid_argument("null incidence array");
+  }
+  const bool neighbors = index.neighbor_offsets != nullptr || index.neighbor_ids != nullptr;
+  if (neighbors && (index.neighbor_offsets == nullptr || (index.neighbor_capacity > 0 && index.neighbor_ids == nullptr))) {
+    throw std::invalid_argument("null neighbour array");
+  }
+  return neighbors;
+}
+
 }  // namespace
 }  // namespace msb
 
@@ -1819,6 +1934,110 @@ int msb_find_cell_contacts(msb_context* context, const msb_cell_arrays* cells,
     launch_touches_to_cell_contacts(c.touches.p, total, c.ids.p, c.records.p, c.stream);
     check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_cell_contact), cudaMemcpyDeviceToHost, c.stream),
           "copy contacts");
+    sync(c);
+  });
+}
+
+int msb_find_cell_contact_graph(msb_context* context, const msb_cell_arrays* cells,
+                                const msb_contact_parameters* parameters, msb_cell_contact* contacts,
+                                uint64_t capacity, uint64_t* count, msb_contact_graph_index* index) {
+  return guarded(context, [&] {
+    if (cells == nullptr || parameters == nullptr || count == nullptr) throw std::invalid_argument("null argument");
+    validate_contact_parameters(*parameters);
+    auto& c = *context;
+    load_cells(c, *cells, false);
+    const ContactSearchParams prm{parameters->activation_margin, parameters->parallel_sine_threshold,
+                                  parameters->degeneracy_epsilon};
+    const std::uint32_t total = find_pairs(c, c.state, prm, c.touches);
+    *count = total;
+    if (total > capacity) throw CapacityError("contact array is too small");
+    if (total > 0 && contacts == nullptr) throw std::invalid_argument("null contact array");
+    const bool neighbors = index != nullptr && check_index(*index, total);
+    c.records.ensure(std::max<std::uint64_t>(total, 1) * sizeof(msb_cell_contact));
+    if (total > 0) launch_touches_to_cell_contacts(c.touches.p, total, c.ids.p, c.records.p, c.stream);
+    if (index != nullptr) {
+      const GraphArrays g = graph_staging(c, cells->count, 2ull * total, neighbors);
+      const std::uint64_t packed = build_graph(c, c.records.p, total, cells->count, false, g);
+      if (neighbors) {
+        index->neighbor_count = packed;
+        if (packed > index->neighbor_capacity) throw CapacityError("neighbour id array is too small");
+      }
+      copy_graph_out(c, g, cells->count, 2ull * total, packed, *index);
+    }
+    if (total > 0) {
+      check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_cell_contact), cudaMemcpyDeviceToHost,
+                            c.stream),
+            "copy contacts");
+    }
+    sync(c);
+  });
+}
+
+int msb_build_contact_graph(msb_context* context, const msb_cell_contact* contacts, uint64_t count,
+                            uint64_t cell_count, uint32_t device_pointers, msb_contact_graph_index* index) {
+  return guarded(context, [&] {
+    if (index == nullptr || (count > 0 && contacts == nullptr)) throw std::invalid_argument("null argument");
+    const bool neighbors = check_index(*index, count);
+    check_graph_size(cell_count, count, false);
+    auto& c = *context;
+    const void* source = contacts;
+    if (device_pointers == 0 && count > 0) {
+      c.graph_contacts.ensure(count * sizeof(msb_cell_contact));
+      check(cudaMemcpyAsync(c.graph_contacts.p, contacts, count * sizeof(msb_cell_contact), cudaMemcpyHostToDevice,
+                            c.stream),
+            "copy contacts");
+      source = c.graph_contacts.p;
+    }
+    GraphArrays g{};
+    if (device_pointers != 0) {
+      g = {index->incidence_offsets, index->incidence_contacts, neighbors ? index->neighbor_offsets : nullptr,
+           index->neighbor_ids, index->neighbor_capacity};
+    } else {
+      g = graph_staging(c, cell_count, 2 * count, neighbors);
+    }
+    const std::uint64_t packed = build_graph(c, source, count, cell_count, false, g);
+    if (neighbors) {
+      index->neighbor_count = packed;
+      if (packed > index->neighbor_capacity) throw CapacityError("neighbour id array is too small");
+    }
+    if (device_pointers == 0) {
+      copy_graph_out(c, g, cell_count, 2 * count, packed, *index);
+    } else {
+      sync(c);
+    }
+  });
+}
+
+int msb_build_external_contact_graph(msb_context* context, const msb_external_contact* contacts, uint64_t count,
+                                     uint64_t cell_count, uint32_t device_pointers, uint64_t* incidence_offsets,
+                                     uint64_t* incidence_contacts) {
+  return guarded(context, [&] {
+    if (count > 0 && contacts == nullptr) throw std::invalid_argument("null argument");
+    if (incidence_offsets == nullptr || (count > 0 && incidence_contacts == nullptr)) {
+      throw std::invalid_argument("null incidence array");
+    }
+    check_graph_size(cell_count, count, true);
+    auto& c = *context;
+    const void* source = contacts;
+    if (device_pointers == 0 && count > 0) {
+      c.graph_contacts.ensure(count * sizeof(msb_external_contact));
+      check(cudaMemcpyAsync(c.graph_contacts.p, contacts, count * sizeof(msb_external_contact),
+                            cudaMemcpyHostToDevice, c.stream),
+            "copy contacts");
+      source = c.graph_contacts.p;
+    }
+    GraphArrays g{};
+    if (device_pointers != 0) {
+      g.incidence_offsets = incidence_offsets;
+      g.incidence = incidence_contacts;
+    } else {
+      g = graph_staging(c, cell_count, count, false);
+    }
+    build_graph(c, source, count, cell_count, true, g);
+    if (device_pointers == 0) {
+      copy_out(c, incidence_offsets, g.incidence_offsets, (cell_count + 1) * 8);
+      copy_out(c, incidence_contacts, g.incidence, count * 8);
+    }
     sync(c);
   });
 }

@@ -13,6 +13,7 @@ from __future__ import annotations
 import numpy as np
 
 from .backend import B200Backend
+from .graph import ContactGraph, ExternalContactGraph
 from .types import (
     ConstraintContactParameters,
     ContactDynamicsParameters,
@@ -92,11 +93,15 @@ class Simulation:
         self._time += float(dt)
         return result
 
-    def find_cell_contacts(self, parameters: ContactParameters | None = None) -> np.ndarray:
-        return self.backend.find_cell_contacts(self.world, parameters)
+    def find_cell_contacts(self, parameters: ContactParameters | None = None) -> ContactGraph:
+        """Simulation::find_cell_contacts: the ContactGraph of the cells."""
+        return self.backend.find_cell_contact_graph(self.world, parameters)
 
-    def find_external_contacts(self, parameters: ConstraintContactParameters | None = None) -> np.ndarray:
-        return self.backend.find_external_contacts(self.world, self.constraints, parameters, every_face=False)
+    def find_external_contacts(self, parameters: ConstraintContactParameters | None = None) -> ExternalContactGraph:
+        """Simulation::find_external_contacts: the ExternalContactGraph of the
+        cells against the constraints."""
+        contacts = self.backend.find_external_contacts(self.world, self.constraints, parameters, every_face=False)
+        return self.backend.build_external_contact_graph(contacts, len(self.world))
 
     def solve_contact_system(self, system: ContactSystem, initial_multipliers,
                              parameters: ContactSolveParameters | None = None) -> ContactSolveResult:

@@ -278,6 +278,32 @@ class Reference(_Checker):
         )
         return offsets, indices[: int(offsets[-1])]
 
+    def contact_graph(self, contacts, cell_count):
+        """ContactGraph(cell_count, contacts): (incidence offsets, incidence
+        contact indices, neighbour offsets, neighbour ids)."""
+        records = np.ascontiguousarray(contacts, dtype=abi.CELL_CONTACT_DTYPE)
+        entries = max(1, 2 * len(records))
+        incidence_offsets = np.zeros(int(cell_count) + 1, dtype=np.uint64)
+        incidence = np.zeros(entries, dtype=np.uint64)
+        neighbor_offsets = np.zeros(int(cell_count) + 1, dtype=np.uint64)
+        neighbors = np.zeros(entries, dtype=np.uint64)
+        count = c_uint64(0)
+        self._call("contact_graph", c_void_p(abi.ptr(records)), c_uint64(len(records)), c_uint64(cell_count),
+                   c_void_p(abi.ptr(incidence_offsets)), c_void_p(abi.ptr(incidence)),
+                   c_void_p(abi.ptr(neighbor_offsets)), c_void_p(abi.ptr(neighbors)), c_uint64(entries),
+                   ctypes.byref(count))
+        return incidence_offsets, incidence[: 2 * len(records)], neighbor_offsets, neighbors[: count.value]
+
+    def external_contact_graph(self, contacts, cell_count):
+        """ExternalContactGraph(cell_count, contacts): (incidence offsets,
+        incidence contact indices)."""
+        records = np.ascontiguousarray(contacts, dtype=abi.EXTERNAL_CONTACT_DTYPE)
+        offsets = np.zeros(int(cell_count) + 1, dtype=np.uint64)
+        indices = np.zeros(max(1, len(records)), dtype=np.uint64)
+        self._call("external_contact_graph", c_void_p(abi.ptr(records)), c_uint64(len(records)),
+                   c_uint64(cell_count), c_void_p(abi.ptr(offsets)), c_void_p(abi.ptr(indices)))
+        return offsets, indices[: len(records)]
+
     def find_cell_contact_candidates(self, world, parameters=None):
         parameters = parameters or ContactParameters()
         cells = world.arrays()

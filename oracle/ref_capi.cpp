@@ -293,6 +293,76 @@ int ref_find_cell_contacts(const msb_cell_arrays* cells, const msb_contact_param
   });
 }
 
+// ContactGraph(cell_count, contacts) (cpp/core/contact_graph.cpp:302-349) on
+// a caller's contact list: its incidence and neighbour arrays, packed.
+int ref_contact_graph(const msb_cell_contact* contacts, uint64_t count, uint64_t cell_count,
+                      uint64_t* incidence_offsets, uint64_t* incidence_contacts, uint64_t* neighbor_offsets,
+                      uint64_t* neighbor_ids, uint64_t neighbor_capacity, uint64_t* neighbor_count) {
+  return guarded([&] {
+    std::vector<ms::CellContact> list(count);
+    for (std::uint64_t i = 0; i < count; ++i) {
+      const auto& c = contacts[i];
+      auto& r = list[i];
+      r.first_id = c.first_id;
+      r.second_id = c.second_id;
+      r.first_slot = c.first_slot;
+      r.second_slot = c.second_slot;
+      r.ordinal = static_cast<std::uint8_t>(c.ordinal);
+      r.point_on_first = {c.point_on_first.x, c.point_on_first.y, c.point_on_first.z};
+      r.normal = {c.normal.x, c.normal.y, c.normal.z};
+      r.signed_separation = c.signed_separation;
+      r.weight = c.weight;
+    }
+    const ms::ContactGraph graph(cell_count, std::move(list));
+    std::uint64_t incident = 0;
+    std::uint64_t neighbors = 0;
+    incidence_offsets[0] = 0;
+    neighbor_offsets[0] = 0;
+    for (std::uint64_t slot = 0; slot < cell_count; ++slot) {
+      for (const auto index : graph.incident_contact_indices(static_cast<ms::Slot>(slot))) {
+        incidence_contacts[incident++] = index;
+      }
+      incidence_offsets[slot + 1] = incident;
+      for (const auto id : graph.neighbor_ids(static_cast<ms::Slot>(slot))) {
+        if (neighbors < neighbor_capacity) neighbor_ids[neighbors] = id;
+        ++neighbors;
+      }
+      neighbor_offsets[slot + 1] = neighbors;
+    }
+    *neighbor_count = neighbors;
+  });
+}
+
+// ExternalContactGraph(cell_count, contacts) (cpp/core/constraints.cpp:288-307).
+int ref_external_contact_graph(const msb_external_contact* contacts, uint64_t count, uint64_t cell_count,
+                               uint64_t* incidence_offsets, uint64_t* incidence_contacts) {
+  return guarded([&] {
+    std::vector<ms::ExternalContact> list(count);
+    for (std::uint64_t i = 0; i < count; ++i) {
+      const auto& c = contacts[i];
+      auto& r = list[i];
+      r.cell_id = c.cell_id;
+      r.cell_slot = c.cell_slot;
+      r.constraint_id = c.constraint_id;
+      r.constraint_kind = static_cast<ms::ExternalConstraintKind>(c.constraint_kind);
+      r.location = static_cast<ms::RodContactLocation>(c.location);
+      r.point_on_cell = {c.point_on_cell.x, c.point_on_cell.y, c.point_on_cell.z};
+      r.normal = {c.normal.x, c.normal.y, c.normal.z};
+      r.signed_separation = c.signed_separation;
+      r.weight = c.weight;
+    }
+    const ms::ExternalContactGraph graph(cell_count, std::move(list));
+    std::uint64_t incident = 0;
+    incidence_offsets[0] = 0;
+    for (std::uint64_t slot = 0; slot < cell_count; ++slot) {
+      for (const auto index : graph.incident_contact_indices(static_cast<ms::Slot>(slot))) {
+        incidence_contacts[incident++] = index;
+      }
+      incidence_offsets[slot + 1] = incident;
+    }
+  });
+}
+
 int ref_find_cell_contact_candidates(const msb_cell_arrays* cells,
                                      const msb_contact_parameters* parameters, uint32_t* pairs,
                                      uint64_t capacity, uint64_t* count) {

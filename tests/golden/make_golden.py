@@ -15,6 +15,13 @@ Cases (each saved as an .npz of input arrays and the reference's outputs):
                     inside and outside, nearest-face and every-face contacts
   chain_*           the make_chain solves of the reference's dynamics
                     conformance test (tests/conformance/contact_dynamics_conformance_test.cpp:56-109)
+  contact_graph     ContactGraph / ExternalContactGraph index arrays
+                    (cpp/core/contact_graph.cpp:302-349, constraints.cpp:288-307)
+                    of colony_1k's contacts and walls, as found and shuffled,
+                    a hand-made list with repeated partners and empty slots,
+                    and the reference's error text for invalid contacts
+
+``python tests/golden/make_golden.py contact_graph`` makes only the named cases.
 """
 
 from __future__ import annotations
@@ -187,11 +194,82 @@ def chain_system(count: int, law: int) -> ContactSystem:
     return ContactSystem(rows, bodies, 0.05, GrowthLoadResponse(law, 0.3, 0.2, 3.0))
 
 
-def main() -> None:
+def hand_made_contacts() -> np.ndarray:
+    """Five cells (slots 0-4, ids 10-14) with slot 3 untouched and two
+    contacts (ordinals 0, 1) between the same pair, listed out of order."""
+    rows = [(11, 14, 1, 4, 0), (10, 12, 0, 2, 0), (10, 12, 0, 2, 1), (12, 14, 2, 4, 0), (10, 11, 0, 1, 0)]
+    out = np.zeros(len(rows), dtype=abi.CELL_CONTACT_DTYPE)
+    for i, (first_id, second_id, first_slot, second_slot, ordinal) in enumerate(rows):
+        out[i]["first_id"], out[i]["second_id"] = first_id, second_id
+        out[i]["first_slot"], out[i]["second_slot"], out[i]["ordinal"] = first_slot, second_slot, ordinal
+        out[i]["normal"] = (0.0, 1.0, 0.0)
+        out[i]["weight"] = 1.0
+        out[i]["signed_separation"] = -0.01
+    return out
+
+
+# Invalid contacts: (field, value) planted in contact 7 of colony_1k's list,
+# with contact 11 broken too so that the lowest failing contact must win.
+GRAPH_ERRORS = (("first_id", 0), ("second_id", 1), ("second_slot", 1000), ("first_slot", 3), ("ordinal", 2),
+                ("weight", 0.0), ("signed_separation", float("nan")), ("normal", (0.0, 0.0, 1.001)))
+EXTERNAL_ERRORS = (("cell_id", 0), ("constraint_id", 0), ("cell_slot", 1000), ("constraint_kind", 4),
+                   ("location", 3), ("weight", -1.0), ("point_on_cell", (float("inf"), 0.0, 0.0)),
+                   ("normal", (0.0, 0.999, 0.0)))
+
+
+def contact_graph_payload(ref) -> dict:
+    colony = np.load(OUT / "colony_1k.npz")
+    walls = np.load(OUT / "walls.npz")
+    cell_count = len(colony["world__ids"])
+    rng = np.random.default_rng(7)
+    payload = {"cell_count": np.int64(cell_count)}
+    # colony_1k's contacts_0.1 and walls' walls_1_0.1 are the lists of the
+    # found and walls cases; the shuffled ones are stored as permutations.
+    found = colony["contacts_0.1"]
+    order = rng.permutation(len(found))
+    payload["shuffled__order"] = order
+    cases = {"found": found, "shuffled": found[order], "hand_made": hand_made_contacts(),
+             "empty": np.zeros(0, dtype=abi.CELL_CONTACT_DTYPE)}
+    counts = {"found": cell_count, "shuffled": cell_count, "hand_made": 8, "empty": 3}
+    for name, contacts in cases.items():
+        if name in ("hand_made", "empty"):
+            payload[f"{name}__contacts"] = contacts
+        payload[f"{name}__cell_count"] = np.int64(counts[name])
+        for key, value in zip(("incidence_offsets", "incidence", "neighbor_offsets", "neighbors"),
+                              ref.contact_graph(contacts, counts[name])):
+            payload[f"{name}__{key}"] = value
+    external = walls["walls_1_0.1"]
+    wall_order = rng.permutation(len(external))
+    payload["walls_shuffled__order"] = wall_order
+    for name, contacts in (("walls", external), ("walls_shuffled", external[wall_order])):
+        offsets, indices = ref.external_contact_graph(contacts, cell_count)
+        payload[f"{name}__incidence_offsets"] = offsets
+        payload[f"{name}__incidence"] = indices
+    for group, errors, base, build in (("cell_error", GRAPH_ERRORS, found, ref.contact_graph),
+                                       ("external_error", EXTERNAL_ERRORS, external, ref.external_contact_graph)):
+        messages = []
+        for field, value in errors:
+            bad = base.copy()
+            bad[7][field] = value
+            bad[11]["weight"] = -2.0
+            try:
+                build(bad, cell_count)
+                messages.append("")
+            except ValueError as error:
+                messages.append(str(error))
+        payload[f"{group}__messages"] = np.array(messages)
+    return payload
+
+
+def main(only: set[str] | None = None) -> None:
     from oracle.native import Reference, build
 
     build(reference=True)
     ref = Reference()
+    if only is not None:
+        if "contact_graph" in only:
+            np.savez_compressed(OUT / "contact_graph.npz", **contact_graph_payload(ref))
+        return
 
     worlds = geometry_kat_worlds()
     payload = {}
@@ -255,9 +333,10 @@ def main() -> None:
         payload[f"{key}__gaps"] = ref.evaluate_contact_gaps(system, solved.multipliers)
         payload[f"{key}__bound"] = np.float32(ref.contact_system_diagonal_bound(system))
     np.savez_compressed(OUT / "chains.npz", **payload)
+    np.savez_compressed(OUT / "contact_graph.npz", **contact_graph_payload(ref))
     for path in sorted(OUT.glob("*.npz")):
         print(path.name, path.stat().st_size)
 
 
 if __name__ == "__main__":
-    main()
+    main(set(sys.argv[1:]) or None)

@@ -142,7 +142,7 @@ def test_closed_chamber_fills_and_holds(sim):
     assert abs(footprint(sim.world) - filled) < 0.02
     cover = footprint(sim.world) / 16.0
     assert 0.6 < cover < 1.0
-    contacts = sim.find_cell_contacts()
+    contacts = sim.find_cell_contacts().contacts
     assert np.all(contacts["signed_separation"] > -0.01)
     assert np.all(np.abs(sim.world.position_x) <= 2.0) and np.all(np.abs(sim.world.position_y) <= 2.0)
     assert np.all(np.abs(sim.world.position_z) < 1e-3)

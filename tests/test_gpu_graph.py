@@ -1,0 +1,164 @@
+"""The contact graph index on the device (msb_build_contact_graph,
+msb_find_cell_contact_graph, msb_build_external_contact_graph) against the
+reference constructors' golden fixture and the numpy oracle: incidence and
+neighbour arrays equal element for element, the reference's error texts, and
+the reference's Python-level ContactGraph behaviour."""
+
+import numpy as np
+import pytest
+
+from microsimulator_b200 import abi, workloads
+from microsimulator_b200.simulation import Simulation
+from microsimulator_b200.types import ContactParameters
+from oracle import graph_oracle
+from tests.golden.make_golden import EXTERNAL_ERRORS, GRAPH_ERRORS
+from tests.test_oracle_graph import graph_cases, random_contacts
+
+pytestmark = pytest.mark.gpu
+
+
+def assert_graph(graph, expected, count):
+    offsets, incidence, neighbor_offsets, neighbors = expected
+    assert np.array_equal(graph.incidence_offsets, offsets)
+    assert np.array_equal(graph.incidence_contacts, incidence)
+    assert np.array_equal(graph.neighbor_offsets, neighbor_offsets)
+    assert np.array_equal(graph.packed_neighbor_ids, neighbors)
+    assert len(graph) == count
+
+
+def test_graph_of_fixture_lists_is_the_references(backend, golden):
+    data, lists = graph_cases(golden)
+    for name, contacts in lists.items():
+        cell_count = int(data[f"{name}__cell_count"])
+        graph = backend.build_contact_graph(contacts, cell_count)
+        expected = [data[f"{name}__{key}"] for key in ("incidence_offsets", "incidence", "neighbor_offsets",
+                                                       "neighbors")]
+        assert_graph(graph, expected, len(contacts))
+        assert graph.cell_count == cell_count
+
+
+def test_found_contact_graph_is_the_references(backend, golden):
+    data, lists = graph_cases(golden)
+    colony = golden("colony_1k")
+    from tests.golden.make_golden import world_from
+
+    world = world_from(colony, "world__")
+    graph = backend.find_cell_contact_graph(world, ContactParameters(activation_margin=0.1))
+    assert np.array_equal(graph.contacts.view(np.uint8), lists["found"].view(np.uint8))
+    expected = [data[f"found__{key}"] for key in ("incidence_offsets", "incidence", "neighbor_offsets",
+                                                  "neighbors")]
+    assert_graph(graph, expected, len(lists["found"]))
+
+
+def test_external_graph_is_the_references(backend, golden):
+    data = golden("contact_graph")
+    walls = golden("walls")["walls_1_0.1"]
+    for name, contacts in (("walls", walls), ("walls_shuffled", walls[data["walls_shuffled__order"]])):
+        graph = backend.build_external_contact_graph(contacts, int(data["cell_count"]))
+        assert np.array_equal(graph.incidence_offsets, data[f"{name}__incidence_offsets"])
+        assert np.array_equal(graph.incidence_contacts, data[f"{name}__incidence"])
+
+
+@pytest.mark.parametrize("group", ["cell_error", "external_error"])
+def test_invalid_contacts_raise_the_references_text(backend, golden, group):
+    data = golden("contact_graph")
+    cell_count = int(data["cell_count"])
+    if group == "cell_error":
+        errors, base, build = GRAPH_ERRORS, golden("colony_1k")["contacts_0.1"], backend.build_contact_graph
+    else:
+        errors, base, build = EXTERNAL_ERRORS, golden("walls")["walls_1_0.1"], backend.build_external_contact_graph
+    for (field, value), message in zip(errors, data[f"{group}__messages"]):
+        bad = base.copy()
+        bad[7][field] = value
+        bad[11]["weight"] = -2.0
+        with pytest.raises(ValueError) as error:
+            build(bad, cell_count)
+        assert str(error.value) == message, field
+
+
+@pytest.mark.parametrize("cells,count", [(2, 1), (7, 40), (300, 2000), (5000, 400), (70_000, 300_000)])
+def test_random_lists_match_the_oracle(backend, cells, count):
+    rng = np.random.default_rng(cells + count)
+    contacts = random_contacts(rng, cells, count)
+    graph = backend.build_contact_graph(contacts, cells + 3)
+    assert_graph(graph, graph_oracle.contact_graph(contacts, cells + 3), count)
+
+
+def test_large_colony_graph_matches_the_oracle(backend):
+    world = workloads.jammed(200_000, seed=3)
+    graph = backend.find_cell_contact_graph(world, ContactParameters(activation_margin=0.05))
+    assert len(graph) > 300_000
+    assert_graph(graph, graph_oracle.contact_graph(graph.contacts, len(world)), len(graph.contacts))
+    # size-independent properties: every contact listed under both its slots,
+    # each neighbour list strictly ascending
+    assert graph.incidence_offsets[-1] == 2 * len(graph)
+    for slot in range(0, len(world), 997):
+        ids = graph.neighbor_ids(slot)
+        assert all(a < b for a, b in zip(ids, ids[1:]))
+
+
+def test_device_pointers(backend):
+    torch = pytest.importorskip("torch")
+    import ctypes
+
+    rng = np.random.default_rng(5)
+    contacts = random_contacts(rng, 1000, 5000)
+    cells = 1000
+    device = torch.device("cuda", 0)
+    records = torch.from_numpy(contacts.view(np.uint8).copy()).to(device)
+    arrays = {name: torch.zeros(n, dtype=torch.int64, device=device) for name, n in (
+        ("incidence_offsets", cells + 1), ("incidence_contacts", 2 * len(contacts)),
+        ("neighbor_offsets", cells + 1), ("neighbor_ids", 2 * len(contacts)))}
+    index = abi.ContactGraphIndex()
+    for name, tensor in arrays.items():
+        setattr(index, name, tensor.data_ptr())
+    index.neighbor_capacity = 2 * len(contacts)
+    torch.cuda.synchronize()
+    backend._check(backend._lib.msb_build_contact_graph(backend._handle, records.data_ptr(), len(contacts), cells, 1,
+                                                       ctypes.byref(index)))
+    expected = graph_oracle.contact_graph(contacts, cells)
+    got = [arrays[name].cpu().numpy().view(np.uint64) for name in ("incidence_offsets", "incidence_contacts",
+                                                                    "neighbor_offsets", "neighbor_ids")]
+    got[3] = got[3][: index.neighbor_count]
+    for mine, other in zip(got, expected):
+        assert np.array_equal(mine, other)
+
+
+def test_neighbor_capacity_is_reported(backend):
+    import ctypes
+
+    contacts = random_contacts(np.random.default_rng(9), 50, 300)
+    graph = graph_oracle.contact_graph(contacts, 50)
+    offsets = np.zeros(51, dtype=np.uint64)
+    incidence = np.zeros(600, dtype=np.uint64)
+    neighbor_offsets = np.zeros(51, dtype=np.uint64)
+    neighbors = np.zeros(4, dtype=np.uint64)
+    index = abi.ContactGraphIndex()
+    index.incidence_offsets, index.incidence_contacts = abi.ptr(offsets), abi.ptr(incidence)
+    index.neighbor_offsets, index.neighbor_ids = abi.ptr(neighbor_offsets), abi.ptr(neighbors)
+    index.neighbor_capacity = 4
+    status = backend._lib.msb_build_contact_graph(backend._handle, ctypes.c_void_p(abi.ptr(contacts)), len(contacts),
+                                                  50, 0, ctypes.byref(index))
+    assert status == abi.ERR_CAPACITY
+    assert index.neighbor_count == len(graph[3])
+
+
+def test_contact_graph_through_the_simulation_api(backend):
+    """The reference's test_contact_graph_is_available_through_the_public_api
+    (python/tests/test_simulation.py:243-271), on this backend."""
+    sim = Simulation(backend=backend)
+    sim.add_cell(position=(0.0, 0.0, 0.0), length=4.0, radius=0.5)
+    sim.add_cell(position=(0.0, 0.8, 0.0), length=4.0, radius=0.5)
+    graph = sim.find_cell_contacts(ContactParameters())
+    assert graph.cell_count == 2
+    assert not graph.empty
+    assert len(graph) == 2
+    assert graph.incident_contact_indices(0) == [0, 1]
+    assert graph.neighbor_ids(0) == [2]
+    assert graph.neighbor_ids(1) == [1]
+    assert graph.contacts["ordinal"].tolist() == [0, 1]
+    assert np.allclose(graph.contacts["signed_separation"], -0.2, atol=1e-6)
+    with pytest.raises(IndexError):
+        graph.neighbor_ids(2)
+    with pytest.raises(IndexError):
+        graph.incident_contact_indices(5)
