@@ -59,6 +59,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--no-learned", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
+    p.add_argument("--no-graph", action="store_true")
     p.add_argument("--sweep-colonies", type=int, default=256)
     p.add_argument("--train-cells", type=int, default=200_000)
     p.add_argument("--train-steps", type=int, default=1500)
@@ -239,6 +240,66 @@ def reference_arm(args):
         "cpu_baseline": sample,
         "e2e": {"value": sample["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def contact_graph_arm(backend, world, local, with_cpu):
+    """The contact graph index (ContactGraph's constructor) of the colony's
+    contacts: the C-ABI call on device-resident contacts (wall clock around
+    the synchronous call, which reads the validation result once), the
+    host-buffer call, and the reference constructor on the same list."""
+    import torch
+
+    from microsimulator_b200.graph import device_index
+
+    contacts = backend.find_cell_contacts(world)
+    n, count = len(world), len(contacts)
+    device = torch.device("cuda", local)
+    records = torch.from_numpy(contacts.view(np.uint8).copy()).to(device)
+    index, _arrays = device_index(n, 2 * count, device)
+    torch.cuda.synchronize()
+
+    def call():
+        backend.build_contact_graph_device(records.data_ptr(), count, n, index)
+
+    for _ in range(3):
+        call()
+    times = []
+    for _ in range(10):
+        t0 = time.perf_counter()
+        call()
+        times.append(time.perf_counter() - t0)
+    device_ms = float(np.median(times)) * 1e3
+    host_times = []
+    for _ in range(4):
+        t0 = time.perf_counter()
+        graph = backend.build_contact_graph(contacts, n)
+        host_times.append(time.perf_counter() - t0)
+    host_ms = float(np.median(host_times[1:])) * 1e3
+    packed = int(index.neighbor_count)
+    # Every field of every contact is read (validation), the incidence and
+    # neighbour ids and both offset arrays written once.
+    algorithmic = count * 64 + 2 * count * 8 + packed * 8 + 2 * (n + 1) * 8
+    peak, peak_kind = measured_peak()
+    achieved = algorithmic / (device_ms * 1e-3) / 1e9
+    out = {"workload": f"the contacts of the jammed colony after the timed steps (margin 0), {count} contacts, "
+                       f"{n} cells", "contacts": count, "cells": n, "neighbor_ids": packed,
+           "device_call_ms": device_ms, "host_buffer_call_ms": host_ms, "algorithmic_bytes": algorithmic,
+           "achieved_gbs": achieved, "frac": achieved / peak, "peak_kind": f"{peak_kind} hbm_gbs",
+           "check": bool(graph.incidence_offsets[-1] == 2 * count and len(graph.packed_neighbor_ids) == packed)}
+    if with_cpu:
+        from oracle.native import REFERENCE_PATH, Reference
+
+        if REFERENCE_PATH.exists():
+            ref = Reference()
+            ref_times = []
+            for _ in range(2):
+                t0 = time.perf_counter()
+                ref.contact_graph(contacts, n)
+                ref_times.append(time.perf_counter() - t0)
+            out["cpu_baseline"] = {"ms": min(ref_times) * 1e3, "cores": ref.thread_count(), "kind": "reference",
+                                   "sample": "ContactGraph(cell_count, contacts) on the same list, "
+                                             "including the driver's copies in and out"}
+    return out
 
 
 def learned_arm(args, backend, snapshot, timed, device_step, local, rank, barrier, dist):
@@ -474,6 +535,10 @@ def main():
         e2e = {"value": e2e_all / e2e_total, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
+    graph_line = None
+    if not args.no_graph and world_size == 1:
+        graph_line = contact_graph_arm(backend, world, local, with_cpu=not args.no_cpu)
+
     sweep_line = None
     if not args.no_sweep:
         sweep_line = sweep_arm(args, backend, local, rank, dist)
@@ -517,6 +582,7 @@ def main():
             "bb_iterations_per_step": iterations / args.steps,
             "learned": learned,
             "sweep": sweep_line,
+            "contact_graph": graph_line,
             "phase_ms_per_step": phases,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",

@@ -195,6 +195,14 @@ class B200Backend:
                                                       cell_count, 0, ctypes.byref(index)))
         return self._graph(cell_count, records.copy(), index, arrays)
 
+    def build_contact_graph_device(self, contacts_pointer: int, count: int, cell_count: int, index) -> int:
+        """msb_build_contact_graph on device-resident contact records and
+        index arrays (``graph.device_index``); returns the packed neighbour
+        id count."""
+        self._check(self._lib.msb_build_contact_graph(self._handle, c_void_p(contacts_pointer), count, cell_count, 1,
+                                                      ctypes.byref(index)))
+        return int(index.neighbor_count)
+
     def build_external_contact_graph(self, contacts: np.ndarray, cell_count: int) -> ExternalContactGraph:
         """ExternalContactGraph(cell_count, contacts) (constraints.cpp:288-307)."""
         records = np.ascontiguousarray(contacts, dtype=abi.EXTERNAL_CONTACT_DTYPE)

@@ -1565,14 +1565,7 @@ constexpr const char* kExternalContactReasons[] = {
     "external contact normal is not unit length",
 };
 
-// Index arrays in device memory.
-struct GraphArrays {
-  std::uint64_t* incidence_offsets;
-  std::uint64_t* incidence;
-  std::uint64_t* neighbor_offsets;  // null: no neighbour index
-  std::uint64_t* neighbors;
-  std::uint64_t neighbor_capacity;
-};
+using GraphArrays = GraphIndexArrays;
 
 void check_graph_size(std::uint64_t cell_count, std::uint64_t count, bool external) {
   // checked_offset_count (contact_graph.cpp:209-215)
@@ -1587,22 +1580,20 @@ void check_graph_size(std::uint64_t cell_count, std::uint64_t count, bool extern
 std::uint64_t build_graph(Ctx& c, const void* contacts, std::uint64_t count, std::uint64_t cell_count,
                           bool external, const GraphArrays& out) {
   check_graph_size(cell_count, count, external);
+  const std::uint64_t entries = external ? count : 2 * count;
   c.graph_words.ensure(4);
-  launch_validate_contacts(contacts, count, cell_count, external, c.graph_words.p, c.stream);
-  unsigned long long words[2] = {0, 0};
+  c.graph_scratch.ensure(graph_scratch_words(entries, cell_count));
+  launch_validate_contacts(contacts, count, cell_count, external, c.graph_words.p, c.graph_scratch.p, c.stream);
+  unsigned long long words[4] = {0, 0, 0, 0};
   check(cudaMemcpyAsync(words, c.graph_words.p, sizeof(words), cudaMemcpyDeviceToHost, c.stream), "copy words");
   sync(c);
   if (words[0] != ~0ull) {
     const unsigned reason = std::min(unsigned(words[0] & 0xFFu), 5u);
     throw std::invalid_argument(external ? kExternalContactReasons[reason] : kCellContactReasons[reason]);
   }
-  const std::uint64_t entries = external ? count : 2 * count;
-  c.graph_scratch.ensure(graph_scratch_words(entries));
-  build_incidence(contacts, count, cell_count, external, out.incidence_offsets, out.incidence, c.graph_scratch.p,
-                  c.stream);
+  build_graph_index(contacts, count, cell_count, external, words[1], words[3], out, c.graph_scratch.p,
+                    c.graph_words.p, c.stream);
   if (external || out.neighbor_offsets == nullptr) return 0;
-  build_neighbors(contacts, count, cell_count, words[1], out.incidence_offsets, out.neighbor_offsets, out.neighbors,
-                  out.neighbor_capacity, c.graph_scratch.p, c.graph_words.p + 2, c.stream);
   unsigned long long total = 0;
   check(cudaMemcpyAsync(&total, c.graph_words.p + 2, sizeof(total), cudaMemcpyDeviceToHost, c.stream),
         "copy count");

@@ -65,3 +65,21 @@ class ContactGraph(ExternalContactGraph):
         (contact_graph.cpp:386-394)."""
         s = self._slot(slot, "contact neighbor slot is out of range")
         return self.packed_neighbor_ids[self.neighbor_offsets[s]:self.neighbor_offsets[s + 1]].tolist()
+
+
+def device_index(cell_count: int, entries: int, device):
+    """Device arrays for a graph index (torch int64 tensors on `device`) and
+    the msb_contact_graph_index that points at them, for calls with
+    device_pointers = 1.  Returns (index, tensors)."""
+    import torch
+
+    from . import abi
+
+    tensors = {name: torch.zeros(max(1, size), dtype=torch.int64, device=device) for name, size in (
+        ("incidence_offsets", cell_count + 1), ("incidence_contacts", entries), ("neighbor_offsets", cell_count + 1),
+        ("neighbor_ids", entries))}
+    index = abi.ContactGraphIndex()
+    for name, tensor in tensors.items():
+        setattr(index, name, tensor.data_ptr())
+    index.neighbor_capacity = entries
+    return index, tensors

@@ -24,6 +24,11 @@ step's own displacement as the guess (warm-start flag 2) and with carried
 forces (flag 1); prints the iterations of each solve of each:
 
   python -m microsimulator_b200.profile_case --case guess --cells 1000000 --warm 3 --steps 3
+
+--case graph: the contact graph index (msb_build_contact_graph) of a jammed
+colony's contacts after `--steps` steps, from device-resident contacts:
+
+  python -m microsimulator_b200.profile_case --case graph --cells 1000000 --steps 1 --iterations 5
 """
 
 from __future__ import annotations
@@ -139,9 +144,38 @@ def guess_case(args) -> None:
     backend.close()
 
 
+def graph_case(args) -> None:
+    """The contact graph index of a settled jammed colony's contacts, built
+    `--iterations` times from device-resident contacts."""
+    import time
+
+    import torch
+
+    from . import workloads
+    from .backend import B200Backend
+    from .graph import device_index
+    from .types import ContactDynamicsParameters
+
+    backend = B200Backend(0)
+    world = workloads.jammed(n=args.cells, seed=args.seed)
+    for _ in range(args.steps):
+        backend.advance_contact_dynamics(world, None, 0.02, ContactDynamicsParameters(overlap_tolerance=5e-4))
+    contacts = backend.find_cell_contacts(world)
+    records = torch.from_numpy(contacts.view(np.uint8).copy()).to("cuda:0")
+    index, _ = device_index(len(world), 2 * len(contacts), "cuda:0")
+    torch.cuda.synchronize()
+    times = []
+    for _ in range(args.iterations):
+        t0 = time.perf_counter()
+        packed = backend.build_contact_graph_device(records.data_ptr(), len(contacts), len(world), index)
+        times.append((time.perf_counter() - t0) * 1e3)
+    print(json.dumps({"cells": len(world), "contacts": len(contacts), "neighbor_ids": packed, "call_ms": times}))
+    backend.close()
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
-    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess"])
+    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess", "graph"])
     p.add_argument("--warm", type=int, default=3)
     p.add_argument("--colonies", type=int, default=64)
     p.add_argument("--cells", type=int, default=500_000)
@@ -157,6 +191,9 @@ def main() -> None:
         return
     if args.case == "guess":
         guess_case(args)
+        return
+    if args.case == "graph":
+        graph_case(args)
         return
 
     from . import workloads

@@ -76,12 +76,30 @@ def test_invalid_contacts_raise_the_references_text(backend, golden, group):
         assert str(error.value) == message, field
 
 
-@pytest.mark.parametrize("cells,count", [(2, 1), (7, 40), (300, 2000), (5000, 400), (70_000, 300_000)])
+# (3, 500) and (40, 3000) put more than 64 entries in a slot: the radix path.
+@pytest.mark.parametrize("cells,count", [(2, 1), (7, 40), (3, 500), (40, 3000), (300, 2000), (5000, 400),
+                                         (70_000, 300_000)])
 def test_random_lists_match_the_oracle(backend, cells, count):
     rng = np.random.default_rng(cells + count)
     contacts = random_contacts(rng, cells, count)
     graph = backend.build_contact_graph(contacts, cells + 3)
     assert_graph(graph, graph_oracle.contact_graph(contacts, cells + 3), count)
+
+
+@pytest.mark.parametrize("hub", [64, 65])
+def test_segment_limit(backend, hub):
+    """A slot with exactly the per-slot sort's limit of entries, and one more."""
+    rng = np.random.default_rng(hub)
+    contacts = random_contacts(rng, 2000, 3000)
+    spokes = random_contacts(rng, 2000, hub)
+    spokes["first_slot"], spokes["first_id"] = 0, 1 + (1 << 33)
+    spokes["second_slot"] = np.arange(1, hub + 1)
+    spokes["second_id"] = spokes["second_slot"].astype(np.uint64) + 1 + (1 << 33)
+    contacts = contacts[(contacts["first_slot"] != 0) & (contacts["second_slot"] != 0)]
+    contacts = np.concatenate([contacts[:1000], spokes, contacts[1000:]])
+    graph = backend.build_contact_graph(contacts, 2000)
+    assert len(graph.incident_contact_indices(0)) == hub
+    assert_graph(graph, graph_oracle.contact_graph(contacts, 2000), len(contacts))
 
 
 def test_large_colony_graph_matches_the_oracle(backend):

@@ -70,7 +70,7 @@ def random_contacts(rng, cells, count):
     return out
 
 
-@pytest.mark.parametrize("cells,count", [(2, 1), (7, 40), (300, 2000), (5000, 400)])
+@pytest.mark.parametrize("cells,count", [(2, 1), (7, 40), (3, 500), (300, 2000), (5000, 400)])
 def test_oracle_matches_the_live_reference(reference, cells, count):
     rng = np.random.default_rng(cells + count)
     contacts = random_contacts(rng, cells, count)
