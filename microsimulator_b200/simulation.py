@@ -106,27 +106,3 @@ class Simulation:
     def solve_contact_system(self, system: ContactSystem, initial_multipliers,
                              parameters: ContactSolveParameters | None = None) -> ContactSolveResult:
         return self.backend.solve_contact_forces(system, initial_multipliers, parameters)
-
-
-def contact_incidence(contacts: np.ndarray, cell_count: int) -> tuple[np.ndarray, np.ndarray]:
-    """ContactGraph's incidence (cpp/core/contact_graph.cpp:316-330): per slot,
-    the indices of its contacts in contact order, as CSR (offsets, indices)."""
-    first = contacts["first_slot"].astype(np.int64)
-    second = contacts["second_slot"].astype(np.int64)
-    index = np.arange(len(contacts), dtype=np.int64)
-    slots = np.stack([first, second], axis=1).reshape(-1)
-    entries = np.stack([index, index], axis=1).reshape(-1)
-    order = np.argsort(slots, kind="stable")
-    counts = np.bincount(slots, minlength=cell_count)
-    offsets = np.zeros(cell_count + 1, dtype=np.int64)
-    np.cumsum(counts, out=offsets[1:])
-    return offsets, entries[order]
-
-
-def neighbor_ids(contacts: np.ndarray, cell_count: int) -> list[list[int]]:
-    """ContactGraph::neighbor_ids: each cell's distinct partners, sorted."""
-    partners: list[set[int]] = [set() for _ in range(cell_count)]
-    for c in contacts:
-        partners[int(c["first_slot"])].add(int(c["second_id"]))
-        partners[int(c["second_slot"])].add(int(c["first_id"]))
-    return [sorted(p) for p in partners]

@@ -6,7 +6,6 @@ import numpy as np
 import pytest
 
 from microsimulator_b200 import abi, workloads
-from microsimulator_b200.simulation import contact_incidence
 from microsimulator_b200.types import ConstraintContactParameters, ContactParameters
 from microsimulator_b200.world import WorldState
 from tests.golden.make_golden import wall_set, world_from
@@ -44,9 +43,10 @@ def test_colony_contacts_and_incidence(backend, golden):
     world = world_from(data, "world__")
     actual = backend.find_cell_contacts(world, ContactParameters(activation_margin=0.1))
     assert actual.tobytes() == data["contacts_0.1"].tobytes()
-    offsets, indices = contact_incidence(actual, len(world))
-    assert np.array_equal(offsets, data["incidence_offsets"].astype(np.int64))
-    assert np.array_equal(indices, data["incidence_indices"].astype(np.int64))
+    graph = backend.find_cell_contact_graph(world, ContactParameters(activation_margin=0.1))
+    assert graph.contacts.tobytes() == data["contacts_0.1"].tobytes()
+    assert np.array_equal(graph.incidence_offsets, data["incidence_offsets"])
+    assert np.array_equal(graph.incidence_contacts, data["incidence_indices"])
 
 
 def test_walls_bit_exact(backend, golden):
