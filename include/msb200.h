@@ -216,7 +216,7 @@ typedef struct msb_contact_dynamics_parameters {
   uint32_t max_iterations;
   uint32_t max_refinements;
   uint32_t max_step_halvings;
-  uint32_t flow_drift; /* must be 0: the flow-drift coupling is not part of this backend */
+  uint32_t flow_drift; /* 1: cells drift with the flow field of msb_set_flow_field (the batch call takes 0) */
   msb_growth_load_response growth;
 } msb_contact_dynamics_parameters;
 

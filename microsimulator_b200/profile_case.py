@@ -110,8 +110,10 @@ def guess_case(args) -> None:
         torch.cuda.synchronize()
         cells.download(w)
         w.next_id = int(w.ids.max()) + 1
+        solves = backend.last_step_solves()
         return {"ms": round(start.elapsed_time(end), 2), "iterations": report.iterations,
-                "solves": backend.last_step_solves()["iterations"].tolist()}
+                "solves": solves["iterations"].tolist(), "rows": solves["rows"].tolist(),
+                "max_overlap": report.max_overlap}
 
     def divide(w, k):
         plan = workloads.plan_divisions(w, 0.02, seed=args.seed * 100003 + k)
@@ -132,6 +134,11 @@ def guess_case(args) -> None:
         exact[:, 2] = np.arctan2(before.direction_x * world.direction_y - before.direction_y * world.direction_x,
                                  before.direction_x * world.direction_x + before.direction_y * world.direction_y)
         guessed = run(before.copy(), 2, exact)
+        # The upper bound of any start of the multipliers: the step run once
+        # with carry-over on (it remembers its own final forces), then the
+        # same step again from the same state starting from them.
+        run(before.copy(), 1)
+        own = run(before.copy(), 1)
         carried_world = previous.copy()
         divide(carried_world, k - 1)
         run(carried_world, 1)  # the previous step, remembered
@@ -140,7 +147,7 @@ def guess_case(args) -> None:
         backend.set_warm_start(0)
         previous = undivided
         print(json.dumps({"step": k, "cells": len(before), "plain": plain, "exact_guess": guessed,
-                          "carried": carried}))
+                          "own_final_forces": own, "carried": carried}))
     backend.close()
 
 
