@@ -60,6 +60,9 @@ def parse():
     p.add_argument("--no-learned", action="store_true")
     p.add_argument("--no-sweep", action="store_true")
     p.add_argument("--no-graph", action="store_true")
+    p.add_argument("--no-walls", action="store_true")
+    p.add_argument("--wall-cells", type=int, default=100_000)
+    p.add_argument("--wall-steps", type=int, default=10)
     p.add_argument("--sweep-colonies", type=int, default=256)
     p.add_argument("--train-cells", type=int, default=200_000)
     p.add_argument("--train-steps", type=int, default=1500)
@@ -240,6 +243,82 @@ def reference_arm(args):
         "cpu_baseline": sample,
         "e2e": {"value": sample["value"], "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }))
+
+
+def walls_arm(args, backend, local, with_cpu):
+    """Capsules at area fraction 0.7 in a trap opening onto a channel with
+    the trap-channel device's wall boxes (100,000 by default), growth 0.5
+    (+1 %/step), every cell of length >= 4 um divided before a step (daughter
+    turns +-0.02 rad).  Device-resident steps timed with CUDA events; beside
+    them the reference CPU backend on the same workload."""
+    import torch
+
+    from microsimulator_b200 import workloads
+    from microsimulator_b200.backend import DeviceCells
+
+    world, walls = workloads.trap_colony(n=args.wall_cells, seed=args.seed)
+    dyn = dynamics()
+
+    def divide_long(w, k):
+        plan = workloads.plan_divisions(w, 1.0, seed=args.seed * 7919 + k, minimum_length=4.0)
+        w.divide_many(plan.parents, 0.5, plan.rotations)
+        return plan
+
+    def step(w, k):
+        divide_long(w, k)
+        cells = DeviceCells(w, device=f"cuda:{local}")
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record()
+        report = backend.advance_contact_dynamics_device(cells, walls, DT, dyn)
+        end.record()
+        torch.cuda.synchronize()
+        cells.download(w)
+        w.next_id = int(w.ids.max()) + 1
+        return start.elapsed_time(end), report
+
+    for k in range(3):
+        step(world, k)
+    snapshot = world.copy()
+    total_ms, cell_steps, iterations, rows = 0.0, 0, 0, 0
+    for k in range(args.wall_steps):
+        ms, report = step(world, 3 + k)
+        total_ms += ms
+        cell_steps += len(world)
+        iterations += report.iterations
+        rows = max(rows, report.max_rows)
+    out = {"workload": f"{args.wall_cells} capsules, lengths U[2, 4] um, area fraction 0.7 in a trap opening onto a "
+                       "channel (trap-channel device wall boxes, 100 x 40 um trap aspect scaled to hold them), "
+                       "growth 0.5, division at 4 um, dt 0.02, tol 5e-4 um",
+           "walls": len(walls), "cells_after": len(world), "steps": args.wall_steps,
+           "value": cell_steps / (total_ms * 1e-3), "unit": "cell-steps/s", "ms_per_step": total_ms / args.wall_steps,
+           "bb_iterations_per_step": iterations / args.wall_steps, "max_rows": rows}
+    if with_cpu:
+        from oracle.native import REFERENCE_PATH, Reference
+
+        if REFERENCE_PATH.exists():
+            ref = Reference()
+            plan_world = snapshot.copy()
+            handle = ref.world_create(plan_world, walls)
+            try:
+                elapsed, ref_cells, ref_steps = 0.0, 0, 0
+                while ref_steps < min(3, args.wall_steps) and (elapsed < 20.0 or ref_steps == 0):
+                    plan = divide_long(plan_world, 3 + ref_steps)
+                    ref.world_divide(handle, plan.parents, plan.rotations)
+                    t0 = time.perf_counter()
+                    ref.world_step(handle, DT, dyn)
+                    elapsed += time.perf_counter() - t0
+                    ref.world_read(handle, plan_world)
+                    plan_world.next_id = int(plan_world.ids.max()) + 1
+                    ref_cells += len(plan_world)
+                    ref_steps += 1
+                out["cpu_baseline"] = {"value": ref_cells / elapsed, "unit": "cell-steps/s",
+                                       "cores": ref.thread_count(), "kind": "reference",
+                                       "sample": f"the first {ref_steps} timed steps of the same workload, "
+                                                 f"{elapsed:.1f} s"}
+            finally:
+                ref.world_destroy(handle)
+    return out
 
 
 def contact_graph_arm(backend, world, local, with_cpu):
@@ -535,6 +614,10 @@ def main():
         e2e = {"value": e2e_all / e2e_total, "unit": "cell-steps/s",
                "h2d_bytes_per_step": h2d // args.steps, "d2h_bytes_per_step": d2h // args.steps}
 
+    walls_line = None
+    if not args.no_walls and world_size == 1:
+        walls_line = walls_arm(args, backend, local, with_cpu=not args.no_cpu)
+
     graph_line = None
     if not args.no_graph and world_size == 1:
         graph_line = contact_graph_arm(backend, world, local, with_cpu=not args.no_cpu)
@@ -583,6 +666,7 @@ def main():
             "learned": learned,
             "sweep": sweep_line,
             "contact_graph": graph_line,
+            "walls": walls_line,
             "phase_ms_per_step": phases,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",

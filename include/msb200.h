@@ -422,6 +422,20 @@ typedef struct msb_solve_record {
 int msb_last_step_solves(const msb_context* context, msb_solve_record* records, uint32_t capacity,
                          uint32_t* count);
 
+/* The form of the BB relaxation on the device (no counterpart in the
+ * reference, whose CUDA backend synchronises with the host every iteration,
+ * cpp/cuda/cuda_backend.cu:1397-1400):
+ *   0  automatic (the default): 1, which measures faster at every size;
+ *   1  a CUDA graph: bound, initial gaps, then a WHILE node repeating a body
+ *      pass and a row pass kernel, whose last block sets the condition;
+ *   2  fused: one persistent cooperative kernel runs the whole solve, with
+ *      two grid barriers per iteration (bounded waits; a wait that runs out
+ *      fails the call with MSB_ERR_DEVICE_CHECK).
+ * Both run the same arithmetic per pass and converge to the same tolerance;
+ * the block count they reduce the BB products over can differ, so step
+ * lengths can differ in the last bits. */
+int msb_set_relaxation(msb_context* context, uint32_t form);
+
 /* Warm starts of the stepper, extensions with no counterpart in the
  * reference (whose stepper starts every step from zero multipliers and keeps
  * no state between steps, contact_dynamics.cpp:725).  `mode` ORs flags:

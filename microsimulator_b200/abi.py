@@ -343,6 +343,7 @@ SIGNATURES = {
         c_int,
         [c_void_p, POINTER(CellArrays), POINTER(ContactParameters), c_void_p, c_uint64, POINTER(c_uint64)],
     ),
+    "msb_set_relaxation": (c_int, [c_void_p, c_uint32]),
     "msb_find_cell_contact_graph": (
         c_int,
         [c_void_p, POINTER(CellArrays), POINTER(ContactParameters), c_void_p, c_uint64, POINTER(c_uint64),

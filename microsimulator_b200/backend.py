@@ -80,6 +80,16 @@ class B200Backend:
     def launch_count(self) -> int:
         return int(self._lib.msb_launch_count(self._handle))
 
+    RELAXATION_AUTOMATIC = 0
+    RELAXATION_GRAPH = 1
+    RELAXATION_FUSED = 2
+
+    def set_relaxation(self, form: int) -> None:
+        """The BB relaxation's form on the device: 0 automatic, 1 a CUDA
+        graph with a WHILE node (two kernels per iteration), 2 one persistent
+        cooperative kernel with grid barriers."""
+        self._check(self._lib.msb_set_relaxation(self._handle, form))
+
     WARM_START_ZERO = 0
     WARM_START_CARRY = 1
     WARM_START_GUESS = 2

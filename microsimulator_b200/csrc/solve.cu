@@ -40,6 +40,13 @@ namespace {
 #ifndef MSB_ROW_MIN_BLOCKS
 #define MSB_ROW_MIN_BLOCKS 1
 #endif
+#ifndef MSB_RELAX_MIN_BLOCKS
+#define MSB_RELAX_MIN_BLOCKS 3
+#endif
+// Back-off of a barrier wait between polls (0: poll without sleeping).
+#ifndef MSB_BARRIER_SLEEP_NS
+#define MSB_BARRIER_SLEEP_NS 64
+#endif
 constexpr int kBatch = MSB_BODY_BATCH;
 
 
@@ -52,15 +59,33 @@ constexpr int kBatch = MSB_BODY_BATCH;
 // mode 0 and 2 evaluate the multipliers as they are; mode 1 their projection.
 // `Tag` only names a second instance of the same code for the timing hook,
 // so that a profiler can select its launches apart from the solve graph's.
-template <int Tag>
-__global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
-  const SolveDesc& d = *desc;
-  const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
-  const float alpha = d.step;
+// Loads of data that other blocks write during a fused solve go through L2
+// (ld.global.cg): L1 is not coherent across SMs within one launch.
+template <bool Coherent>
+__device__ __forceinline__ float shared_load(const float* p) {
+  if constexpr (Coherent) {
+    return __ldcg(p);
+  } else {
+    return *p;
+  }
+}
+template <bool Coherent>
+__device__ __forceinline__ float4 shared_load(const float4* p) {
+  if constexpr (Coherent) {
+    return __ldcg(p);
+  } else {
+    return *p;
+  }
+}
+
+// The body pass over bodies block, block + blocks, ... of the grid.
+template <bool Coherent>
+__device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
+                                          std::uint32_t blocks) {
   const float* __restrict__ g = d.multipliers;
   const float* __restrict__ gap = d.gaps;
   const std::uint32_t* __restrict__ offsets = d.incidence.offsets;
-  for (std::uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < d.body_count; b += gridDim.x * blockDim.x) {
+  for (std::uint32_t b = block * blockDim.x + threadIdx.x; b < d.body_count; b += blocks * blockDim.x) {
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float load = 0.0f;
     const std::uint32_t begin = offsets[b];
@@ -79,8 +104,8 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
           const std::uint32_t row = __float_as_uint(eb[t].w);
-          gv[t] = g[row];
-          pv[t] = mode == 1 ? gap[row] : 0.0f;
+          gv[t] = shared_load<Coherent>(&g[row]);
+          pv[t] = mode == 1 ? shared_load<Coherent>(&gap[row]) : 0.0f;
         }
       }
 #pragma unroll
@@ -106,14 +131,19 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_
   }
 }
 
-// mode 0: gaps of the initial multipliers and the first residual (sets the
-// graph condition); mode 1: one projected step (sets the condition);
-// mode 2: gaps only.
 template <int Tag>
-__global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
-  SolveDesc& d = *desc;
+__global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
+  const SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
-  const float alpha = d.step;
+  body_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
+}
+
+// The row pass over rows block, block + blocks, ... of the grid; unless
+// mode is 2, the block's BB products, residual and finiteness into
+// d.partials[5 * block ...], reduced in a fixed tree.
+template <bool Coherent>
+__device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
+                                         std::uint32_t blocks) {
   const float dt = d.dt;
   float* __restrict__ g = d.multipliers;
   float* __restrict__ gap = d.gaps;
@@ -123,22 +153,22 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
   // row_gap (cpp/cpu/cpu_contact_dynamics.cpp:149-159): each side's
   // jacobian . velocity - lever * elongation rate, summed in that order.
   const bool project = mode == 1;
-  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    const float gpi = project ? gap[i] : 0.0f;
+  for (std::uint32_t i = block * blockDim.x + threadIdx.x; i < d.row_count; i += blocks * blockDim.x) {
+    const float gi = shared_load<Coherent>(&g[i]);
+    const float gpi = project ? shared_load<Coherent>(&gap[i]) : 0.0f;
     const uint2 s = __ldcs(&d.rows.slots[i]);
     const float4 ra = __ldcs(&d.rows.a[i]);
     const float4 rb = __ldcs(&d.rows.b[i]);
     const float4 rd = __ldcs(&d.rows.d[i]);
-    const float4 va = d.response.a[s.x];
-    const float4 vb = d.response.b[s.x];
+    const float4 va = shared_load<Coherent>(&d.response.a[s.x]);
+    const float4 vb = shared_load<Coherent>(&d.response.b[s.x]);
     const float m = project ? smax(0.0f, gi - alpha * gpi) : gi;
     const float v1[6] = {va.x, va.y, va.z, vb.x, vb.y, vb.z};
     float rate = side_term(ra, rb, v1, va.w);
     if (s.y != kInvalidSlot) {
       const float4 rc = __ldcs(&d.rows.c[i]);
-      const float4 wa = d.response.a[s.y];
-      const float4 wb = d.response.b[s.y];
+      const float4 wa = shared_load<Coherent>(&d.response.a[s.y]);
+      const float4 wb = shared_load<Coherent>(&d.response.b[s.y]);
       const float v2[6] = {wa.x, wa.y, wa.z, wb.x, wb.y, wb.z};
       rate += side_term(rc, rd, v2, wa.w);
     }
@@ -177,19 +207,22 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
     for (int w = 1; w < kSolveThreads / 32; ++w) {
       r = k < 3 ? r + red[k][w] : (k == 3 ? fmax(r, red[k][w]) : fmin(r, red[k][w]));
     }
-    d.partials[5 * blockIdx.x + k] = r;
+    d.partials[5 * block + k] = r;
   }
-  __threadfence();
   __syncthreads();
-  __shared__ bool last;
-  if (threadIdx.x == 0) last = atomicAdd(&d.ticket, 1u) == gridDim.x - 1;
-  __syncthreads();
-  if (!last) return;
+}
 
-  // The last block: combine the partials of every block in block order.
-  __threadfence();
+// One block combines the partials of `blocks` blocks in block order (so the
+// result does not depend on scheduling), sets the next step length, the
+// status and whether to go on (d.proceed), as one iteration of
+// iterate_contact_steps does (cpp/core/contact_solver.hpp:66-82); mode 0
+// judges the initial multipliers.  Returns d.proceed (thread 0).
+__device__ __forceinline__ std::uint32_t decide(SolveDesc& d, std::uint32_t mode, std::uint32_t blocks) {
+  __shared__ double red[5][kSolveThreads / 32];
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
   double t[5] = {0.0, 0.0, 0.0, 0.0, 1.0};
-  for (std::uint32_t p = threadIdx.x; p < gridDim.x; p += blockDim.x) {
+  for (std::uint32_t p = threadIdx.x; p < blocks; p += blockDim.x) {
 #pragma unroll
     for (int k = 0; k < 5; ++k) {
       const double x = __ldcg(&d.partials[5 * p + k]);
@@ -209,7 +242,7 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
     for (int k = 0; k < 5; ++k) red[k][warp] = t[k];
   }
   __syncthreads();
-  if (threadIdx.x != 0) return;
+  if (threadIdx.x != 0) return 0;
   double total[5];
   for (int k = 0; k < 5; ++k) {
     total[k] = red[k][0];
@@ -222,7 +255,7 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
   d.residual = reported;
   std::uint32_t proceed = 0;
   if (mode == 0) {
-    const float bound = __uint_as_float(d.bound_bits);
+    const float bound = __uint_as_float(__ldcg(&d.bound_bits));
     d.bound = bound;
     d.iterations = 0;
     if (!isfinite(bound) || !(bound > 0.0f)) {
@@ -251,7 +284,117 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
     }
   }
   d.proceed = proceed;
-  if (set_condition) cudaGraphSetConditional(cudaGraphConditionalHandle(d.handle), proceed);
+  return proceed;
+}
+
+// mode 0: gaps of the initial multipliers and the first residual (sets the
+// graph condition); mode 1: one projected step (sets the condition);
+// mode 2: gaps only.  The last block to finish decides.
+template <int Tag>
+__global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
+  SolveDesc& d = *desc;
+  const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
+  row_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
+  if (mode == 2) return;
+  __threadfence();
+  __shared__ bool last;
+  if (threadIdx.x == 0) last = atomicAdd(&d.ticket, 1u) == gridDim.x - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const std::uint32_t proceed = decide(d, mode, gridDim.x);
+  if (threadIdx.x == 0 && set_condition) cudaGraphSetConditional(cudaGraphConditionalHandle(d.handle), proceed);
+}
+
+// contact_system_diagonal_bound (cpp/cpu/cpu_contact_dynamics.cpp:247-260):
+// the largest dt * J M J^T + c over rows, as an atomic max of float bits.
+__device__ __forceinline__ void bound_pass(const SolveDesc& d, std::uint32_t* bound_bits, std::uint32_t block,
+                                           std::uint32_t blocks) {
+  float bound = 0.0f;
+  for (std::uint32_t i = block * blockDim.x + threadIdx.x; i < d.row_count; i += blocks * blockDim.x) {
+    const uint2 s = d.rows.slots[i];
+    const float4 ra = d.rows.a[i];
+    const float4 rb = d.rows.b[i];
+    float entry = diagonal(ra, rb, d.bodies.a[s.x], d.bodies.b[s.x]);
+    const float4 rd = d.rows.d[i];
+    if (s.y != kInvalidSlot) entry += diagonal(d.rows.c[i], rd, d.bodies.a[s.y], d.bodies.b[s.y]);
+    bound = smax(bound, d.dt * entry + rd.w);
+  }
+  for (int o = 16; o > 0; o >>= 1) bound = smax(bound, __shfl_down_sync(0xFFFFFFFFu, bound, o));
+  if ((threadIdx.x & 31) == 0 && bound > 0.0f) atomicMax(bound_bits, __float_as_uint(bound));
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+// A grid barrier over `blocks` co-resident blocks.  Thread 0 of each block
+// arrives on a counter; the last to arrive (with `decide_mode` >= 0) first
+// combines the row pass's partials and decides with its whole block, then
+// resets the counter and advances the generation that the others wait on.
+// A wait longer than kBarrierTimeoutNs sets barrier_abort, which every
+// waiting block sees.  Returns false once the solve is aborted.
+__device__ __forceinline__ bool grid_barrier(SolveDesc& d, std::uint32_t blocks, int decide_mode) {
+  __shared__ std::uint32_t generation;
+  __shared__ bool last;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    generation = atomicAdd(&d.barrier_generation, 0u);
+    __threadfence();
+    last = atomicAdd(&d.barrier_count, 1u) + 1u == blocks;
+  }
+  __syncthreads();
+  if (last) {
+    __threadfence();
+    if (decide_mode >= 0) decide(d, std::uint32_t(decide_mode), blocks);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      d.barrier_count = 0;
+      __threadfence();
+      atomicAdd(&d.barrier_generation, 1u);
+    }
+  } else if (threadIdx.x == 0) {
+    const unsigned long long start = global_ns();
+    const volatile std::uint32_t* gen = &d.barrier_generation;
+    const volatile std::uint32_t* abort = &d.barrier_abort;
+    while (*gen == generation && *abort == 0u) {
+      if (global_ns() - start > kBarrierTimeoutNs) {
+        atomicExch(&d.barrier_abort, 1u);
+        break;
+      }
+      if (MSB_BARRIER_SLEEP_NS > 0) __nanosleep(MSB_BARRIER_SLEEP_NS);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *static_cast<const volatile std::uint32_t*>(&d.barrier_abort) == 0u;
+}
+
+// The fused solve: bound -> initial gaps and residual -> while not done
+// { body pass; barrier; row pass; barrier and decision }.  The problem (the
+// arrays and constants) comes as a grid-constant parameter, read from the
+// constant bank; the solver state lives in *state (the same descriptor in
+// device memory).
+__global__ void __launch_bounds__(kSolveThreads, MSB_RELAX_MIN_BLOCKS)
+    relax_kernel(const __grid_constant__ SolveDesc problem, SolveDesc* state) {
+  const std::uint32_t blocks = gridDim.x;
+  bound_pass(problem, &state->bound_bits, blockIdx.x, blocks);
+  if (!grid_barrier(*state, blocks, -1)) return;
+  const volatile SolveDesc* shared = state;
+  // mode 0 evaluates the initial multipliers, mode 1 iterates.
+  std::uint32_t mode = 0;
+  float alpha = 0.0f;
+  for (;;) {
+    body_pass<true>(problem, mode, alpha, blockIdx.x, blocks);
+    if (!grid_barrier(*state, blocks, -1)) return;
+    row_pass<true>(problem, mode, alpha, blockIdx.x, blocks);
+    if (!grid_barrier(*state, blocks, int(mode))) return;
+    if (shared->proceed == 0u) return;
+    mode = 1;
+    alpha = shared->step;
+  }
 }
 
 __global__ void __launch_bounds__(kSolveThreads) bound_kernel(SolveDesc* desc) {
@@ -450,6 +593,21 @@ int SolveGraph::launch(cudaStream_t stream) {
   if (err != cudaSuccess) return err;
   count_launch(4);
   return cudaGraphLaunch(exec_, stream);
+}
+
+int relax_resident_blocks() {
+  int device = 0, sms = kSmCount, per_sm = 0;
+  if (cudaGetDevice(&device) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, relax_kernel, kSolveThreads, 0) != cudaSuccess) return 0;
+  return sms * per_sm;
+}
+
+int launch_relax(const SolveDesc& problem, SolveDesc* desc, int blocks, cudaStream_t stream) {
+  SolveDesc copy = problem;
+  void* args[] = {&copy, &desc};
+  count_launch();
+  return cudaLaunchCooperativeKernel(reinterpret_cast<void*>(relax_kernel), dim3(blocks), dim3(kSolveThreads), args,
+                                     0, stream);
 }
 
 void launch_iteration(SolveDesc* desc, int blocks, cudaEvent_t between, cudaStream_t stream) {

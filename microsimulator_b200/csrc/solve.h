@@ -79,6 +79,10 @@ struct SolveDesc {
   unsigned long long handle;  // cudaGraphConditionalHandle of the WHILE node
   std::uint32_t bound_ticket;
   std::uint32_t bound_bits;
+  // grid barrier of the fused solve (relax_kernel)
+  std::uint32_t barrier_count;
+  std::uint32_t barrier_generation;
+  std::uint32_t barrier_abort;  // a barrier wait ran out of time: every block stops
 };
 
 // Builds the incidence of `rows` over `bodies` bodies.  Scratch: `keys` and
@@ -113,6 +117,19 @@ class SolveGraph {
   SolveDesc* desc_ = nullptr;
   unsigned long long handle_ = 0;
 };
+
+// The fused solve: bound, initial gaps and every projected iteration in ONE
+// cooperative launch of `blocks` co-resident blocks, with two bounded grid
+// barriers per iteration (the last block to reach the second combines the
+// BB products and decides).  The whole descriptor, state included, must be
+// reset before the launch; `problem` is its host copy, passed by value as a
+// kernel parameter.  Returns a CUDA error code.
+int launch_relax(const SolveDesc& problem, SolveDesc* desc, int blocks, cudaStream_t stream);
+// Blocks of relax_kernel that fit on the device at once.
+int relax_resident_blocks();
+// How long a barrier wait may take before the solve stops with
+// barrier_abort set.
+constexpr unsigned long long kBarrierTimeoutNs = 5'000'000'000ull;
 
 // Evaluates the response of desc->multipliers once (no solve), as
 // evaluate_contact_response does; also the gaps when `with_gaps`.
