@@ -13,7 +13,10 @@
 //              does not depend on scheduling), sets the next step length and
 //              the convergence flag, and writes the flag into the WHILE node
 //              of the CUDA graph that repeats the two passes.
-// The host launches the graph once per solve and reads the report once.
+// The host launches the graph once per solve and reads the report once.  The
+// WHILE body holds MSB_WHILE_UNROLL (body, row) pairs; a pair whose solve
+// has already converged returns at once, so the result is that of one pair
+// per evaluation.
 
 #include <algorithm>
 #include <cfloat>
@@ -39,6 +42,13 @@ namespace {
 #endif
 #ifndef MSB_ROW_MIN_BLOCKS
 #define MSB_ROW_MIN_BLOCKS 1
+#endif
+// (body pass, row pass) pairs per WHILE-node body of the solve graph; a pair
+// after the one that converged returns at once.  Fewer evaluations of the
+// WHILE node: per BB iteration, 1 -> 8 pairs measured 116 -> 112 us at 1M
+// capsules, 24.6 -> 21.0 us at 100k, 19.7 -> 16.0 us at 20k.
+#ifndef MSB_WHILE_UNROLL
+#define MSB_WHILE_UNROLL 8
 #endif
 #ifndef MSB_RELAX_MIN_BLOCKS
 #define MSB_RELAX_MIN_BLOCKS 3
@@ -135,6 +145,7 @@ template <int Tag>
 __global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_kernel(SolveDesc* desc, int fixed_mode) {
   const SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
+  if (fixed_mode < 0 && mode == 1 && d.proceed == 0u) return;  // an unrolled pair after convergence
   body_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
 }
 
@@ -294,6 +305,7 @@ template <int Tag>
 __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_kernel(SolveDesc* desc, int fixed_mode, int set_condition) {
   SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
+  if (fixed_mode < 0 && mode == 1 && d.proceed == 0u) return;  // an unrolled pair after convergence
   row_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
   if (mode == 2) return;
   __threadfence();
@@ -579,9 +591,16 @@ int SolveGraph::create(SolveDesc* desc, int blocks, cudaStream_t stream) {
   cp.conditional.size = 1;
   if ((err = cudaGraphAddNode(&loop, graph_, &row0, 1, &cp)) != cudaSuccess) return err;
   cudaGraph_t body = cp.conditional.phGraph_out[0];
-  cudaGraphNode_t body1, row1;
-  if ((err = kernel_node(body, &body1, nullptr, 0, (void*)body_pass_kernel<0>, body_args, blocks)) != cudaSuccess) return err;
-  if ((err = kernel_node(body, &row1, &body1, 1, (void*)row_pass_kernel<0>, row_args, blocks)) != cudaSuccess) return err;
+  cudaGraphNode_t previous = nullptr;
+  for (int pair = 0; pair < MSB_WHILE_UNROLL; ++pair) {
+    cudaGraphNode_t body1, row1;
+    if ((err = kernel_node(body, &body1, previous != nullptr ? &previous : nullptr, previous != nullptr ? 1 : 0,
+                           (void*)body_pass_kernel<0>, body_args, blocks)) != cudaSuccess) {
+      return err;
+    }
+    if ((err = kernel_node(body, &row1, &body1, 1, (void*)row_pass_kernel<0>, row_args, blocks)) != cudaSuccess) return err;
+    previous = row1;
+  }
   err = cudaGraphInstantiate(&exec_, graph_, 0);
   count_launch(0);
   return err;
