@@ -870,8 +870,15 @@ std::uint32_t find_touches(Ctx& c, Geometry& geometry, const msb_contact_paramet
 
 // ---- solve ---------------------------------------------------------------
 
+#ifndef MSB_GRAPH_CLASSES
+#define MSB_GRAPH_CLASSES 1, 4, 16, 74, 148, 296, 444, 592, 1184
+#endif
+
+// The solve graph for a system of `items` rows or bodies: one per class of
+// grid sizes (the smallest class that gives every thread an item, at most
+// one resident wave).
 SolveGraph& graph_for(Ctx& c, std::uint32_t items) {
-  static constexpr int classes[] = {1, 4, 16, 74, 148, 592, 1184};
+  static constexpr int classes[] = {MSB_GRAPH_CLASSES};
   const std::uint32_t wanted = (items + kSolveThreads - 1) / kSolveThreads;
   int index = 0;
   while (index + 1 < int(std::size(classes)) && std::uint32_t(classes[index]) < wanted) ++index;
