@@ -482,6 +482,7 @@ struct msb_context {
   msb::FlowField flow{};
   msb::DBuf<float> flow_x, flow_y, flow_z;
   msb::DBuf<std::uint8_t> flow_obstacles;
+  msb::DBuf<float4> flow_sites;  // per site the sums of its two faces along each axis
   float flow_travel_limit = 0.0f;
   msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
   msb::DBuf<std::uint32_t> inc_offsets;
@@ -1826,7 +1827,12 @@ int msb_set_flow_field(msb_context* context, const msb_flow_field* field) {
     c.flow = {field->shape_x, field->shape_y, field->shape_z,
               make_float3(field->origin.x, field->origin.y, field->origin.z),
               make_float3(field->spacing.x, field->spacing.y, field->spacing.z),
-              c.flow_x.p, c.flow_y.p, c.flow_z.p, obstacles};
+              c.flow_x.p, c.flow_y.p, c.flow_z.p, obstacles, nullptr};
+    c.flow_sites.ensure(std::size_t(field->shape_x) * field->shape_y * field->shape_z);
+    launch_flow_sites(c.flow, c.flow_sites.p, c.stream);
+    c.flow.sites = c.flow_sites.p;
+    check(cudaGetLastError(), "flow sites");
+    sync(c);
     c.flow_travel_limit = 0.25f * std::min({field->spacing.x, field->spacing.y, field->spacing.z});
     c.has_flow = true;
   });

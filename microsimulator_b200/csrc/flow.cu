@@ -57,11 +57,36 @@ __device__ __forceinline__ std::size_t site_of(const FlowField& f, std::uint32_t
   return std::size_t(x) * f.shape_y * f.shape_z + std::size_t(y) * f.shape_z + z;
 }
 
-// SignalGrid::sample_velocity(position, clamped).
+// SignalGrid::sample_velocity(position, clamped).  A site's velocity is the
+// mean of its two faces along each axis, w * 0.5f * (face0 + face1) per
+// axis; the face sums come precomputed per site (the same float additions),
+// so one float4 load replaces six scalar ones.
 __device__ F3 sample_velocity(const FlowField& f, F3 p) {
   const Axis ax = axis_weights(p.x, f.origin.x, f.spacing.x, f.shape_x);
   const Axis ay = axis_weights(p.y, f.origin.y, f.spacing.y, f.shape_y);
   const Axis az = axis_weights(p.z, f.origin.z, f.spacing.z, f.shape_z);
+  if (f.obstacles == nullptr) {
+    // The stencil in the reference's order (x, then y, then z); entries
+    // beyond an axis's count have weight 0 and are skipped, as are zero
+    // weights.
+    F3 r{0.0f, 0.0f, 0.0f};
+#pragma unroll
+    for (int i = 0; i < 2; ++i) {
+#pragma unroll
+      for (int j = 0; j < 2; ++j) {
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+          const float w = ax.weight[i] * ay.weight[j] * az.weight[k];
+          if (w == 0.0f) continue;
+          const float4 s = f.sites[site_of(f, ax.index[i], ay.index[j], az.index[k])];
+          r.x += w * 0.5f * s.x;
+          r.y += w * 0.5f * s.y;
+          r.z += w * 0.5f * s.z;
+        }
+      }
+    }
+    return r;
+  }
   std::uint32_t cx[8], cy[8], cz[8];
   float weight[8];
   std::uint32_t count = 0;
@@ -111,18 +136,30 @@ __device__ F3 sample_velocity(const FlowField& f, F3 p) {
   for (std::uint32_t i = 0; i < count; ++i) {
     const float w = weight[i];
     if (w == 0.0f) continue;
-    const std::uint32_t x = cx[i], y = cy[i], z = cz[i];
+    const float4 s = f.sites[site_of(f, cx[i], cy[i], cz[i])];
+    r.x += w * 0.5f * s.x;
+    r.y += w * 0.5f * s.y;
+    r.z += w * 0.5f * s.z;
+  }
+  return r;
+}
+
+__global__ void flow_sites_kernel(FlowField f, float4* __restrict__ sites) {
+  const std::uint64_t count = std::uint64_t(f.shape_x) * f.shape_y * f.shape_z;
+  for (std::uint64_t s = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; s < count;
+       s += std::uint64_t(gridDim.x) * blockDim.x) {
+    const std::uint32_t z = std::uint32_t(s % f.shape_z);
+    const std::uint32_t y = std::uint32_t((s / f.shape_z) % f.shape_y);
+    const std::uint32_t x = std::uint32_t(s / (std::uint64_t(f.shape_z) * f.shape_y));
     const std::size_t xf0 = std::size_t(x) * f.shape_y * f.shape_z + std::size_t(y) * f.shape_z + z;
     const std::size_t xf1 = std::size_t(x + 1) * f.shape_y * f.shape_z + std::size_t(y) * f.shape_z + z;
     const std::size_t yf0 = std::size_t(x) * (f.shape_y + 1) * f.shape_z + std::size_t(y) * f.shape_z + z;
     const std::size_t yf1 = std::size_t(x) * (f.shape_y + 1) * f.shape_z + std::size_t(y + 1) * f.shape_z + z;
     const std::size_t zf0 = std::size_t(x) * f.shape_y * (f.shape_z + 1) + std::size_t(y) * (f.shape_z + 1) + z;
     const std::size_t zf1 = zf0 + 1;
-    r.x += w * 0.5f * (f.x_faces[xf0] + f.x_faces[xf1]);
-    r.y += w * 0.5f * (f.y_faces[yf0] + f.y_faces[yf1]);
-    r.z += w * 0.5f * (f.z_faces[zf0] + f.z_faces[zf1]);
+    sites[s] = make_float4(f.x_faces[xf0] + f.x_faces[xf1], f.y_faces[yf0] + f.y_faces[yf1],
+                           f.z_faces[zf0] + f.z_faces[zf1], 0.0f);
   }
-  return r;
 }
 
 // Simulation::flow_derivative(point, axis, lambda, rotates = true).
@@ -209,6 +246,13 @@ __global__ void flow_speed_kernel(std::uint32_t n, GeometryBuffers state, const 
 }
 
 }  // namespace
+
+void launch_flow_sites(const FlowField& field, float4* sites, cudaStream_t stream) {
+  const std::uint64_t count = std::uint64_t(field.shape_x) * field.shape_y * field.shape_z;
+  if (count == 0) return;
+  flow_sites_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(field, sites);
+  count_launch();
+}
 
 void launch_flow_drift(std::uint32_t n, GeometryBuffers state, const std::uint8_t* fixed, const FlowField& field,
                        float dt, BodyArrays bodies, std::uint32_t* status, cudaStream_t stream) {

@@ -11,7 +11,8 @@
 namespace msb {
 
 // A velocity field on a lattice of sites (device pointers): face velocities
-// x-major as the reference's signal grid stores them, optional solid mask.
+// x-major as the reference's signal grid stores them, optional solid mask,
+// and per site the sums of its two faces along each axis (launch_flow_sites).
 struct FlowField {
   std::uint32_t shape_x, shape_y, shape_z;
   float3 origin;
@@ -20,7 +21,11 @@ struct FlowField {
   const float* y_faces;
   const float* z_faces;
   const std::uint8_t* obstacles;  // null: no obstacles
+  const float4* sites;            // (x0 + x1, y0 + y1, z0 + z1, 0) per site
 };
+
+// The per-site face sums of `field` into `sites` (one float4 per site).
+void launch_flow_sites(const FlowField& field, float4* sites, cudaStream_t stream);
 
 // Writes each body's drift (drift_a: velocity, drift_b: angular velocity)
 // for a substep of length dt from the geometry in `state`; fixed cells get

@@ -29,6 +29,11 @@ forces (flag 1); prints the iterations of each solve of each:
 colony's contacts after `--steps` steps, from device-resident contacts:
 
   python -m microsimulator_b200.profile_case --case graph --cells 1000000 --steps 1 --iterations 5
+
+--case trap: steps of the trap colony with its wall boxes, drifting in a
+slow swirl (flow drift on), so that every kernel of a step runs:
+
+  python -m microsimulator_b200.profile_case --case trap --cells 300000 --steps 2
 """
 
 from __future__ import annotations
@@ -180,9 +185,50 @@ def graph_case(args) -> None:
     backend.close()
 
 
+def trap_case(args) -> None:
+    """Steps of the trap colony (capsules in a trap with the trap-channel
+    device's wall boxes) drifting in a swirling flow: every kernel of the
+    step runs, wall contacts and flow drift included."""
+    import time
+
+    from . import workloads
+    from .backend import B200Backend
+    from .types import ContactDynamicsParameters, FlowField
+
+    backend = B200Backend(0)
+    world, walls = workloads.trap_colony(n=args.cells, seed=args.seed)
+    x = np.concatenate([world.position_x, [0.0]])
+    y = np.concatenate([world.position_y, [0.0]])
+    spacing = 4.0
+    origin = (float(x.min()) - 200.0, float(y.min()) - 200.0, -0.5)
+    shape = (int((x.max() - x.min() + 400.0) / spacing) + 1, int((y.max() - y.min() + 400.0) / spacing) + 1, 1)
+    sx, sy, sz = shape
+    x_faces = np.zeros((sx + 1, sy, sz), np.float32)
+    y_faces = np.zeros((sx, sy + 1, sz), np.float32)
+    z_faces = np.zeros((sx, sy, sz + 1), np.float32)
+    # A slow solid-body swirl, zero on the lattice boundary.
+    xs = origin[0] + spacing * np.arange(sx + 1)
+    ys = origin[1] + spacing * (np.arange(sy) + 0.5)
+    x_faces[1:-1, :, 0] = (-0.002 * (ys[None, :] - ys.mean()) + 0.0 * xs[1:-1, None]).astype(np.float32)
+    xs = origin[0] + spacing * (np.arange(sx) + 0.5)
+    y_faces[:, 1:-1, 0] = (0.002 * (xs[:, None] - xs.mean())).astype(np.float32)
+    backend.set_flow_field(FlowField(shape, origin, (spacing, spacing, 1.0), x_faces, y_faces, z_faces, None))
+    dyn = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    for step in range(args.steps):
+        plan = workloads.plan_divisions(world, 1.0, seed=args.seed * 7919 + step, minimum_length=4.0)
+        world.divide_many(plan.parents, 0.5, plan.rotations)
+        t0 = time.perf_counter()
+        result = backend.advance_contact_dynamics(world, walls, 0.02, dyn)
+        world.next_id = int(world.ids.max()) + 1
+        print(json.dumps({"step": step, "cells": len(world), "ms": round(1e3 * (time.perf_counter() - t0), 2),
+                          "iterations": result.report.iterations, "substeps": result.report.substeps,
+                          "phases": backend.last_step_phases()}))
+    backend.close()
+
+
 def main() -> None:
     p = argparse.ArgumentParser()
-    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess", "graph"])
+    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess", "graph", "trap"])
     p.add_argument("--warm", type=int, default=3)
     p.add_argument("--colonies", type=int, default=64)
     p.add_argument("--cells", type=int, default=500_000)
@@ -201,6 +247,9 @@ def main() -> None:
         return
     if args.case == "graph":
         graph_case(args)
+        return
+    if args.case == "trap":
+        trap_case(args)
         return
 
     from . import workloads
