@@ -310,15 +310,22 @@ namespace msb {
 // (pageable cudaMemcpy goes through the driver's single bounce buffer).
 class HostCopies {
  public:
+  // A host copy of `bytes` from src to dst.  With `ready`, the copy first
+  // waits for that event (a download's DMA into src).  With `device`, the
+  // copy is followed by a DMA of dst to device on `stream` (an upload's
+  // chunk starts on its way as soon as it is staged).
   struct Job {
     void* dst;
     const void* src;
     std::size_t bytes;
+    cudaEvent_t ready = nullptr;
+    void* device = nullptr;
+    cudaStream_t stream = nullptr;
   };
 
   HostCopies() {
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
-    const unsigned helpers = std::min(7u, hw > 1 ? hw - 1 : 0u);
+    const unsigned helpers = std::min(15u, hw > 1 ? hw - 1 : 0u);
     for (unsigned t = 0; t < helpers; ++t) threads_.emplace_back([this] { serve(); });
   }
   HostCopies(const HostCopies&) = delete;
@@ -333,17 +340,20 @@ class HostCopies {
   }
 
   // Runs every job (split into chunks) on the pool and this thread; returns
-  // when all are done.
-  void run(const std::vector<Job>& jobs) {
+  // when all are done (and every upload DMA is queued).  Returns the first
+  // CUDA error a chunk met.
+  cudaError_t run(const std::vector<Job>& jobs) {
     chunks_.clear();
+    error_.store(cudaSuccess);
     constexpr std::size_t kChunk = std::size_t(1) << 21;
     for (const auto& j : jobs) {
       for (std::size_t at = 0; at < j.bytes; at += kChunk) {
         const std::size_t len = std::min(kChunk, j.bytes - at);
-        chunks_.push_back({static_cast<char*>(j.dst) + at, static_cast<const char*>(j.src) + at, len});
+        chunks_.push_back({static_cast<char*>(j.dst) + at, static_cast<const char*>(j.src) + at, len, j.ready,
+                           j.device != nullptr ? static_cast<char*>(j.device) + at : nullptr, j.stream});
       }
     }
-    if (chunks_.empty()) return;
+    if (chunks_.empty()) return cudaSuccess;
     {
       std::lock_guard<std::mutex> lock(mutex_);
       next_.store(0);
@@ -354,14 +364,22 @@ class HostCopies {
     work();
     std::unique_lock<std::mutex> lock(mutex_);
     done_.wait(lock, [this] { return busy_ == 0; });
+    return error_.load();
   }
 
  private:
+  void fail(cudaError_t e) {
+    cudaError_t expected = cudaSuccess;
+    if (e != cudaSuccess) error_.compare_exchange_strong(expected, e);
+  }
   void work() {
     for (;;) {
       const std::size_t k = next_.fetch_add(1);
       if (k >= chunks_.size()) return;
-      std::memcpy(chunks_[k].dst, chunks_[k].src, chunks_[k].bytes);
+      const Job& j = chunks_[k];
+      if (j.ready != nullptr) fail(cudaEventSynchronize(j.ready));
+      std::memcpy(j.dst, j.src, j.bytes);
+      if (j.device != nullptr) fail(cudaMemcpyAsync(j.device, j.dst, j.bytes, cudaMemcpyHostToDevice, j.stream));
     }
   }
   void serve() {
@@ -384,6 +402,7 @@ class HostCopies {
   std::vector<std::thread> threads_;
   std::vector<Job> chunks_;
   std::atomic<std::size_t> next_{0};
+  std::atomic<cudaError_t> error_{cudaSuccess};
   std::mutex mutex_;
   std::condition_variable wake_, done_;
   std::size_t busy_ = 0;
@@ -526,7 +545,8 @@ struct msb_context {
   // host-buffer calls: pinned staging both ways and the host-side copy pool
   std::unique_ptr<msb::HostCopies> copies;
   msb::PinnedBuffer upload, download;
-  std::vector<msb::HostCopies::Job> pending;  // download copies to run after the stream syncs
+  std::vector<msb::HostCopies::Job> pending;  // download copies, each waiting for its DMA's event
+  std::vector<cudaEvent_t> download_events;
 
   // phase timing of the last step: events at phase boundaries
   std::vector<cudaEvent_t> phase_events;
@@ -647,14 +667,23 @@ msb::HostCopies& host_copies(Ctx& c) {
 void stage_download(Ctx& c, void* dst, const void* device_src, std::size_t bytes, std::size_t& at) {
   unsigned char* slot = c.download.p + at;
   check(cudaMemcpyAsync(slot, device_src, bytes, cudaMemcpyDeviceToHost, c.stream), "copy back");
-  c.pending.push_back({dst, slot, bytes});
+  // The host copy of this array may start once its own DMA is done.
+  const std::size_t k = c.pending.size();
+  if (k == c.download_events.size()) {
+    cudaEvent_t e;
+    check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    c.download_events.push_back(e);
+  }
+  check(cudaEventRecord(c.download_events[k], c.stream), "event");
+  c.pending.push_back({dst, slot, bytes, c.download_events[k]});
   at += (bytes + 255) & ~std::size_t(255);
 }
 
 void flush_downloads(Ctx& c) {
   if (c.pending.empty()) return;
-  host_copies(c).run(c.pending);
+  const cudaError_t err = host_copies(c).run(c.pending);
   c.pending.clear();
+  check(err, "copy back");
 }
 
 void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
@@ -694,22 +723,18 @@ void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
       check(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyDeviceToDevice, c.stream), "copy cells");
     }
   } else {
-    // Through pinned staging: the host side in parallel, then one DMA per array.
     std::size_t total = 0;
     for (const auto& u : uploads) total += (u.bytes + 255) & ~std::size_t(255);
+    // Through pinned staging: the host side in parallel, each 2 MiB chunk's
+    // DMA queued as soon as it is staged.
     unsigned char* base = c.upload.ensure(total);
     std::vector<msb::HostCopies::Job> host;
     std::size_t at = 0;
     for (const auto& u : uploads) {
-      host.push_back({base + at, u.src, u.bytes});
+      host.push_back({base + at, u.src, u.bytes, nullptr, u.dst, c.stream});
       at += (u.bytes + 255) & ~std::size_t(255);
     }
-    host_copies(c).run(host);
-    at = 0;
-    for (const auto& u : uploads) {
-      check(cudaMemcpyAsync(u.dst, base + at, u.bytes, cudaMemcpyHostToDevice, c.stream), "copy cells");
-      at += (u.bytes + 255) & ~std::size_t(255);
-    }
+    check(host_copies(c).run(host), "copy cells");
   }
   c.state.ensure(n);
   reset_status(c);
@@ -1752,6 +1777,7 @@ void msb_context_destroy(msb_context* context) {
   cudaSetDevice(context->device);
   if (context->stream != nullptr) cudaStreamSynchronize(context->stream);
   for (auto e : context->phase_events) cudaEventDestroy(e);
+  for (auto e : context->download_events) cudaEventDestroy(e);
   context->graphs.clear();
   if (context->desc != nullptr) cudaFree(context->desc);
   if (context->host_scalars != nullptr) cudaFreeHost(context->host_scalars);
@@ -2302,8 +2328,8 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     write_back(c, *cells, device_pointers, at);
     write_outputs(c, outputs, device_pointers, at);
     mark(c, kPhaseEnd);
+    flush_downloads(c);  // each array's host copy starts when its DMA is done
     sync(c);
-    flush_downloads(c);
     collect_phases(c);
     *report = outcome.report;
   });
@@ -2453,8 +2479,8 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     write_back(c, *cells, device_pointers != 0, at);
     write_outputs(c, outputs, device_pointers != 0, at);
     mark(c, kPhaseEnd);
+    flush_downloads(c);  // each array's host copy starts when its DMA is done
     sync(c);
-    flush_downloads(c);
     collect_phases(c);
     *report = outcome.report;
     for (std::uint32_t i = 0; i < colony_count; ++i) {
