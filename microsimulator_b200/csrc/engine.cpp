@@ -2062,8 +2062,8 @@ int msb_build_contact_graph(msb_context* context, const msb_cell_contact* contac
                             uint64_t cell_count, uint32_t device_pointers, msb_contact_graph_index* index) {
   return guarded(context, [&] {
     if (index == nullptr || (count > 0 && contacts == nullptr)) throw std::invalid_argument("null argument");
+    check_graph_size(cell_count, count, false);  // the constructor's first check (contact_graph.cpp:305-306)
     const bool neighbors = check_index(*index, count);
-    check_graph_size(cell_count, count, false);
     auto& c = *context;
     const void* source = contacts;
     if (device_pointers == 0 && count > 0) {
@@ -2098,10 +2098,10 @@ int msb_build_external_contact_graph(msb_context* context, const msb_external_co
                                      uint64_t* incidence_contacts) {
   return guarded(context, [&] {
     if (count > 0 && contacts == nullptr) throw std::invalid_argument("null argument");
+    check_graph_size(cell_count, count, true);
     if (incidence_offsets == nullptr || (count > 0 && incidence_contacts == nullptr)) {
       throw std::invalid_argument("null incidence array");
     }
-    check_graph_size(cell_count, count, true);
     auto& c = *context;
     const void* source = contacts;
     if (device_pointers == 0 && count > 0) {

@@ -124,3 +124,60 @@ def test_flow_drift_needs_a_field(backend):
         bad.x_faces = bad.x_faces.copy()
         bad.x_faces[0, 0, 0] = np.nan
         backend.set_flow_field(bad)
+
+
+def field_3d(shape=(10, 9, 4), spacing=(2.5, 2.5, 1.5), origin=(-5.0, -5.0, -3.0), seed=2, solid=False):
+    """A sheared flow with a vertical component on a 3-D lattice (every face
+    of the boundary closed)."""
+    sx, sy, sz = shape
+    ox, oy, oz = origin
+    hx, hy, hz = spacing
+    rng = np.random.default_rng(seed)
+    xf = np.zeros((sx + 1, sy, sz), np.float32)
+    yf = np.zeros((sx, sy + 1, sz), np.float32)
+    zf = np.zeros((sx, sy, sz + 1), np.float32)
+    for i in range(1, sx):
+        for j in range(sy):
+            for k in range(sz):
+                y, z = oy + (j + 0.5) * hy, oz + (k + 0.5) * hz
+                xf[i, j, k] = 0.2 * y + 0.1 * z + 0.02 * rng.standard_normal()
+    for i in range(sx):
+        for j in range(1, sy):
+            for k in range(sz):
+                x = ox + (i + 0.5) * hx
+                yf[i, j, k] = -0.15 * x + 0.02 * rng.standard_normal()
+    for i in range(sx):
+        for j in range(sy):
+            for k in range(1, sz):
+                x = ox + (i + 0.5) * hx
+                zf[i, j, k] = 0.05 * x + 0.01 * rng.standard_normal()
+    obstacles = None
+    if solid:
+        obstacles = np.zeros((sx, sy, sz), np.uint8)
+        obstacles[6, 2:4, 1:3] = 1
+        for i, j, k in np.argwhere(obstacles):
+            xf[i, j, k] = xf[i + 1, j, k] = 0.0
+            yf[i, j, k] = yf[i, j + 1, k] = 0.0
+            zf[i, j, k] = zf[i, j, k + 1] = 0.0
+    return FlowField(shape, origin, spacing, xf, yf, zf, obstacles)
+
+
+@pytest.mark.parametrize("solid", [False, True])
+def test_drift_on_a_3d_lattice_is_the_references(backend, reference, solid):
+    world = WorldState()
+    world.add_cell(position=(1.0, 2.0, 0.5), direction=(0.6, 0.0, 0.8), length=2.5, growth_rate=0.0)
+    world.add_cell(position=(8.0, 6.0, -1.0), direction=(0.0, 0.6, 0.8), length=1.5, growth_rate=0.0)
+    world.add_cell(position=(12.0, 1.0, 2.2), direction=(1.0, 0.0, 0.0), length=2.0, growth_rate=0.0)
+    world.add_cell(position=(-9.0, 30.0, 9.0), direction=(0.0, 1.0, 0.0), length=2.0, growth_rate=0.0)  # clamped
+    f = field_3d(solid=solid)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        rg = backend.advance_contact_dynamics(gpu, None, DT, p)
+    finally:
+        backend.set_flow_field(None)
+    rr = reference.flow_step(ref, f, DT, p)
+    assert rg.report.substeps == rr.substeps
+    assert np.max(np.abs(gpu.geometry()[:, 2] - world.geometry()[:, 2])) > 1e-5  # vertical drift too
+    assert np.array_equal(gpu.geometry(), ref.geometry()), np.max(np.abs(gpu.geometry() - ref.geometry()))

@@ -180,3 +180,19 @@ def test_contact_graph_through_the_simulation_api(backend):
         graph.neighbor_ids(2)
     with pytest.raises(IndexError):
         graph.incident_contact_indices(5)
+
+
+def test_slot_index_space_and_empty_graphs(backend):
+    import ctypes
+
+    empty = np.zeros(0, dtype=abi.CELL_CONTACT_DTYPE)
+    graph = backend.build_contact_graph(empty, 0)
+    assert graph.cell_count == 0 and graph.empty and graph.incidence_offsets.tolist() == [0]
+    graph = backend.build_contact_graph(empty, 5)
+    assert graph.incidence_offsets.tolist() == [0] * 6 and graph.neighbor_ids(4) == []
+    # checked_offset_count (contact_graph.cpp:209-215): beyond the slot index space.
+    index = abi.ContactGraphIndex()
+    status = backend._lib.msb_build_contact_graph(backend._handle, None, 0, (1 << 32), 0, ctypes.byref(index))
+    assert status == abi.ERR_OVERFLOW
+    external = np.zeros(0, dtype=abi.EXTERNAL_CONTACT_DTYPE)
+    assert backend.build_external_contact_graph(external, 3).incidence_offsets.tolist() == [0, 0, 0, 0]
