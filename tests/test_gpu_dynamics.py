@@ -240,3 +240,28 @@ def test_device_resident_step_equals_host_step(backend):
     assert rh.report == rd
     assert np.array_equal(host.geometry(), device.geometry())
     assert np.array_equal(rh.axial_loads, outputs.loads.cpu().numpy())
+
+
+def test_steps_are_deterministic(backend):
+    """The same step from the same state gives the same bits, on the same
+    context and on a fresh one (the reference's thread-invariance test,
+    tests/cpp/thread_invariance_test.cpp:61-84, asks this across thread
+    counts): every reduction on the device runs in a fixed order."""
+    from microsimulator_b200.backend import B200Backend
+
+    world = workloads.jammed(30_000, seed=17)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4)
+    runs = []
+    for b in (backend, backend, None):
+        fresh = b is None
+        if fresh:
+            b = B200Backend(0)
+        w = world.copy()
+        result = b.advance_contact_dynamics(w, None, 0.02, p)
+        runs.append((w.geometry(), result.report, result.center_velocities, result.axial_loads))
+        if fresh:
+            b.close()
+    for geometry, report, velocities, loads in runs[1:]:
+        assert np.array_equal(geometry, runs[0][0])
+        assert report == runs[0][1]
+        assert np.array_equal(velocities, runs[0][2]) and np.array_equal(loads, runs[0][3])
