@@ -265,3 +265,69 @@ def test_steps_are_deterministic(backend):
         assert np.array_equal(geometry, runs[0][0])
         assert report == runs[0][1]
         assert np.array_equal(velocities, runs[0][2]) and np.array_equal(loads, runs[0][3])
+
+
+def within(actual, expected, tolerance):
+    """trajectory_conformance_test.cpp's comparison: abs + rel tolerance."""
+    return np.all(np.abs(actual - expected) <= tolerance + tolerance * np.abs(expected))
+
+
+def test_trajectory_conformance(backend, reference):
+    """The mechanical part of the reference's trajectory conformance test
+    (tests/conformance/trajectory_conformance_test.cpp:26-172): three cells
+    (one fixed) on a plane, steps of 0.01, 0.015 and 0.02 at overlap
+    tolerance 2e-4, cell 2 divided after the first; geometry within 2e-3
+    (absolute plus relative) of the reference CPU backend after every step."""
+    world = WorldState()
+    positions = [(0.0, 0.0, 0.0), (0.0, 0.65, 0.0), (0.2, 1.3, 0.1)]
+    directions = [(1.0, 0.0, 0.0), (1.0, 0.1, 0.0), (0.95, -0.1, 0.08)]
+    for i in range(3):
+        world.add_cell(position=positions[i], direction=directions[i], length=3.0 + 0.2 * i, radius=0.45,
+                       growth_rate=0.02 + 0.01 * i, fixed=i == 0)
+    walls = ConstraintSet()
+    walls.add_plane(point=(0.0, 0.4, 0.0), inward_normal=(0.0, 1.0, 0.0), coefficient=1.25)
+    p = ContactDynamicsParameters(overlap_tolerance=2.0e-4)
+    handle = reference.world_create(world, walls)
+    try:
+        gpu, mirror = world.copy(), world.copy()
+        for step, dt in enumerate((0.01, 0.015, 0.02)):
+            rg = backend.advance_contact_dynamics(gpu, walls, dt, p).report
+            rr = reference.world_step(handle, dt, p)
+            reference.world_read(handle, mirror)
+            assert within(rg.max_overlap, rr.max_overlap, 2.0e-3)
+            assert np.array_equal(gpu.ids, mirror.ids)
+            assert within(gpu.geometry(), mirror.geometry(), 2.0e-3), np.max(np.abs(gpu.geometry() - mirror.geometry()))
+            if step == 0:
+                identity = np.array([[1.0, 0.0, 1.0, 0.0]], np.float32)
+                gpu.divide_many([2], 0.5, identity)
+                mirror.divide_many([2], 0.5, identity)
+                reference.world_divide(handle, [2], identity)
+                reference.world_read(handle, mirror)
+                assert np.array_equal(gpu.geometry(), mirror.geometry())
+    finally:
+        reference.world_destroy(handle)
+
+
+def test_growing_colony_trajectory(backend, reference):
+    """A colony of 40 cells grown for 25 steps with every cell of length >= 4
+    divided (daughter turns +-0.02 rad), stepped in lockstep with the
+    reference CPU backend: geometry within 2e-3 of it after every step."""
+    world = workloads.colony_1k(seed=23, n=40, side=14.0, growth_rate=0.5)
+    p = ContactDynamicsParameters(overlap_tolerance=2.0e-4)
+    handle = reference.world_create(world)
+    try:
+        gpu, mirror = world.copy(), world.copy()
+        for step in range(25):
+            plan = workloads.plan_divisions(mirror, 1.0, seed=1000 + step, minimum_length=4.0)
+            for w in (gpu, mirror):
+                w.divide_many(plan.parents, 0.5, plan.rotations)
+            reference.world_divide(handle, plan.parents, plan.rotations)
+            backend.advance_contact_dynamics(gpu, None, 0.02, p)
+            reference.world_step(handle, 0.02, p)
+            reference.world_read(handle, mirror)
+            gpu.next_id = mirror.next_id = int(mirror.ids.max()) + 1
+            assert np.array_equal(gpu.ids, mirror.ids)
+            assert within(gpu.geometry(), mirror.geometry(), 2.0e-3), (step, np.max(np.abs(gpu.geometry() - mirror.geometry())))
+        assert len(gpu) > 50  # it grew and divided
+    finally:
+        reference.world_destroy(handle)
