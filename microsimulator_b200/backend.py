@@ -39,8 +39,10 @@ def device_count() -> int:
 class B200Backend:
     """make_cuda_backend(device_index): one context, one stream, its buffers."""
 
-    def __init__(self, device_index: int = 0):
-        self._lib = abi.load_library()
+    def __init__(self, device_index: int = 0, library=None):
+        """`library`: a path to load instead of libmsb200.so (the checked
+        build, ``build.CHECKED_OUTPUT``)."""
+        self._lib = abi.load_library(library)
         handle = c_void_p()
         status = self._lib.msb_context_create(device_index, ctypes.byref(handle))
         if status != abi.OK:

@@ -1,4 +1,7 @@
-"""Builds ``libmsb200.so`` in-tree for sm_100a.
+"""Builds ``libmsb200.so`` in-tree for sm_100a, and its checked twin
+``libmsb200_checked.so`` (``MSB_DEVICE_CHECKS=1``: the hot gathers check
+their indices and report MSB_ERR_DEVICE_CHECK instead of reading out of
+range; for debugging and its own tests, not for timing).
 
 CUDA sources are compiled by nvcc with ``--fmad=false`` (no contracted
 multiply-adds, so FP32 results round like the reference's) and IEEE division
@@ -19,6 +22,7 @@ PACKAGE = Path(__file__).resolve().parent
 CSRC = PACKAGE / "csrc"
 BUILD = PACKAGE / "_build"
 OUTPUT = PACKAGE / "libmsb200.so"
+CHECKED_OUTPUT = PACKAGE / "libmsb200_checked.so"
 INCLUDE = PACKAGE.parent / "include"
 
 CUDA_HOME = Path(os.environ.get("CUDA_HOME", "/usr/local/cuda"))
@@ -53,22 +57,26 @@ def _stale(target: Path, deps) -> bool:
     return any(d.stat().st_mtime > mtime for d in deps)
 
 
-def build(verbose: bool = False, force: bool = False) -> Path:
-    """Compiles every CUDA and C++ source and links the shared library."""
+def build(verbose: bool = False, force: bool = False, checked: bool = False) -> Path:
+    """Compiles every CUDA and C++ source and links the shared library (the
+    checked twin with ``checked``)."""
     if shutil.which(NVCC) is None and not Path(NVCC).exists():
         raise RuntimeError(f"nvcc not found at {NVCC}")
-    BUILD.mkdir(exist_ok=True)
+    build_dir = BUILD / "checked" if checked else BUILD
+    output = CHECKED_OUTPUT if checked else OUTPUT
+    nvcc_flags = [*NVCC_FLAGS, "-DMSB_DEVICE_CHECKS=1"] if checked else NVCC_FLAGS
+    build_dir.mkdir(parents=True, exist_ok=True)
     cu, cpp = _sources()
     headers = list(CSRC.glob("*.h")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
     jobs = []
     objects = []
     for src in cu:
-        obj = BUILD / (src.stem + ".cu.o")
+        obj = build_dir / (src.stem + ".cu.o")
         objects.append(obj)
         if force or _stale(obj, [src, *headers]):
-            jobs.append([NVCC, *NVCC_FLAGS, "-c", str(src), "-o", str(obj)])
+            jobs.append([NVCC, *nvcc_flags, "-c", str(src), "-o", str(obj)])
     for src in cpp:
-        obj = BUILD / (src.stem + ".o")
+        obj = build_dir / (src.stem + ".o")
         objects.append(obj)
         if force or _stale(obj, [src, *headers]):
             jobs.append(["g++", *CXX_FLAGS, "-c", str(src), "-o", str(obj)])
@@ -84,13 +92,13 @@ def build(verbose: bool = False, force: bool = False) -> Path:
             if verbose:
                 print(" ".join(cmd[-3:]), file=sys.stderr)
                 print(log, file=sys.stderr)
-    if force or jobs or _stale(OUTPUT, objects):
+    if force or jobs or _stale(output, objects):
         link = [
             NVCC,
             *ARCH,
             "-shared",
             "-o",
-            str(OUTPUT),
+            str(output),
             *map(str, objects),
             "-cudart=static",
             "-Xcompiler",
@@ -101,7 +109,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         result = subprocess.run(link, capture_output=True, text=True)
         if result.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(link)}\n{result.stdout}\n{result.stderr}")
-    return OUTPUT
+    return output
 
 
 if __name__ == "__main__":

@@ -512,10 +512,15 @@ __device__ F3 deterministic_normal(const Capsule& p, const Capsule& q, const Poi
 
 __global__ void narrow_phase_kernel(GeometryView g, const uint2* __restrict__ pairs, std::uint64_t pair_count,
                                     ContactSearchParams prm, std::uint32_t* __restrict__ counts,
-                                    const std::uint32_t* __restrict__ offsets, Touch* __restrict__ touches) {
+                                    const std::uint32_t* __restrict__ offsets, Touch* __restrict__ touches,
+                                    std::uint32_t* status) {
   for (std::uint64_t k = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; k < pair_count;
        k += std::uint64_t(gridDim.x) * blockDim.x) {
     const uint2 pair = pairs[k];
+    if (!index_ok(pair.x, g.count, status) || !index_ok(pair.y, g.count, status)) {
+      if (counts != nullptr) counts[k] = 0;
+      continue;
+    }
     const Capsule p = capsule_at(g, pair.x);
     const Capsule q = capsule_at(g, pair.y);
     PointPair pts[2];
@@ -1013,10 +1018,11 @@ void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std
 }
 
 void launch_narrow_phase(GeometryView g, const uint2* pairs, std::uint64_t pair_count, ContactSearchParams p,
-                         std::uint32_t* counts, const std::uint32_t* offsets, Touch* touches, cudaStream_t stream) {
+                         std::uint32_t* counts, const std::uint32_t* offsets, Touch* touches, cudaStream_t stream,
+                         std::uint32_t* status) {
   if (pair_count == 0) return;
   narrow_phase_kernel<<<grid_for(pair_count, kThreads, 16), kThreads, 0, stream>>>(g, pairs, pair_count, p, counts,
-                                                                                    offsets, touches);
+                                                                                    offsets, touches, status);
   count_launch();
 }
 

@@ -59,4 +59,20 @@ __device__ __forceinline__ void raise_status(std::uint32_t* status, std::uint32_
   atomicCAS(status, 0u, code);
 }
 
+// Index checks of the checked build (MSB_DEVICE_CHECKS=1, libmsb200_checked.so):
+// an index at or past its bound records kStatusIndex in *status and the
+// caller skips the access.  In the ordinary build the check is compiled out.
+#ifndef MSB_DEVICE_CHECKS
+#define MSB_DEVICE_CHECKS 0
+#endif
+__device__ __forceinline__ bool index_ok(std::uint64_t index, std::uint64_t bound, std::uint32_t* status) {
+  if constexpr (MSB_DEVICE_CHECKS != 0) {
+    if (index >= bound) {
+      if (status != nullptr) raise_status(status, kStatusIndex);
+      return false;
+    }
+  }
+  return true;
+}
+
 }  // namespace msb

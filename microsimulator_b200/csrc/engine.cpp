@@ -26,6 +26,7 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include "../../include/msb200.h"
 #include "batch.h"
@@ -550,6 +551,7 @@ struct msb_context {
 
   // phase timing of the last step: events at phase boundaries
   std::vector<cudaEvent_t> phase_events;
+  bool nvtx_open = false;  // an NVTX range of the current phase is open
   std::vector<int> phase_marks;
   std::vector<msb_solve_record> solve_log;  // the solves of the last step, in order
   std::array<double, 8> phase_ms{};
@@ -584,8 +586,16 @@ enum Phase : int {
   kPhaseEnd = 8
 };
 
-// Records an event on the stream where `phase` begins (the previous phase ends).
+constexpr const char* kPhaseNames[] = {"msb load", "msb search", "msb rows",   "msb incidence",
+                                       "msb solve", "msb move",   "msb output", "msb guess"};
+
+// Records an event on the stream where `phase` begins (the previous phase
+// ends), and opens an NVTX range of the phase's name for profilers (closed
+// at the next mark).
 void mark(Ctx& c, int phase) {
+  if (c.nvtx_open) nvtxRangePop();
+  c.nvtx_open = phase != kPhaseEnd;
+  if (c.nvtx_open) nvtxRangePushA(kPhaseNames[phase]);
   if (c.phase_marks.size() == c.phase_events.size()) {
     cudaEvent_t e;
     check(cudaEventCreate(&e), "event");
@@ -854,13 +864,15 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   c.pair_offsets.ensure(pair_count + 1ull);
   c.temp.ensure(scan_temp_words(pair_count + 1ull) + scan_temp_words(capacity) + sort_temp_words(n) + 64);
   check(cudaMemsetAsync(c.pair_counts.p + pair_count, 0, 4, c.stream), "memset");
-  launch_narrow_phase(g, c.pairs.p, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream);
+  launch_narrow_phase(g, c.pairs.p, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream,
+                      c.scalars.p + kStatus);
   exclusive_scan(c.pair_counts.p, c.pair_offsets.p, pair_count + 1ull, c.temp.p, c.stream);
   const std::uint32_t touch_count = read_u32(c, c.pair_offsets.p + pair_count);
   read_scalars(c);
   if (touch_count == 0) return 0;
   out.ensure(touch_count + 1ull);
-  launch_narrow_phase(g, c.pairs.p, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream);
+  launch_narrow_phase(g, c.pairs.p, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream,
+                      c.scalars.p + kStatus);
   return touch_count;
 }
 
@@ -963,6 +975,7 @@ void fill_desc(Ctx& c, std::uint32_t row_count, float dt, const msb_growth_load_
     d.barrier_count = 0;
     d.barrier_generation = 0;
     d.barrier_abort = 0;
+    d.check_status = 0;
     check(cudaMemcpyAsync(c.desc, &d, sizeof(SolveDesc), cudaMemcpyHostToDevice, c.stream), "desc");
     return;
   }
@@ -980,7 +993,7 @@ void build_system_incidence(Ctx& c, std::uint32_t row_count) {
   c.counts.ensure(c.n + 1ull);
   c.temp.ensure(sort_temp_words(entries) + scan_temp_words(c.n + 1ull) + 64);
   build_incidence(c.rows.arrays(), row_count, c.n, {c.inc_offsets.p, c.inc_a.p, c.inc_b.p}, c.sort_keys.p,
-                  c.sort_values.p, c.counts.p, c.temp.p, c.stream);
+                  c.sort_values.p, c.counts.p, c.temp.p, c.stream, c.scalars.p + kStatus);
 }
 
 void build_row_keys(Ctx& c, RowStore& store) {
@@ -1027,6 +1040,7 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
   sync(c);
   const SolveDesc& d = *c.host_desc;
   if (d.barrier_abort != 0) throw DeviceCheckError("a grid barrier of the relaxation ran out of time");
+  if (d.check_status != 0) throw DeviceCheckError("an index check of the relaxation failed");
   if (!fused) count_launch(int(2 * d.iterations));
   c.solve_log.push_back({rows, d.iterations, d.status, d.residual});
   if (d.status == 3) throw std::invalid_argument("contact system has no positive diagonal");

@@ -143,7 +143,7 @@ void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std
 // (count pass, `touches` null) or the contacts themselves at offsets[pair].
 void launch_narrow_phase(GeometryView g, const uint2* pairs, std::uint64_t pair_count,
                          ContactSearchParams p, std::uint32_t* counts, const std::uint32_t* offsets,
-                         Touch* touches, cudaStream_t stream);
+                         Touch* touches, cudaStream_t stream, std::uint32_t* status = nullptr);
 // Wall contacts of every cell: counts[rank[cell]] (count pass) or the
 // contacts at touch_base + offsets[rank[cell]] (fill pass).  every_face
 // selects find_external_contact_faces over find_external_contacts.

@@ -91,7 +91,7 @@ __device__ __forceinline__ float4 shared_load(const float4* p) {
 // The body pass over bodies block, block + blocks, ... of the grid.
 template <bool Coherent>
 __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
-                                          std::uint32_t blocks) {
+                                          std::uint32_t blocks, std::uint32_t* check) {
   const float* __restrict__ g = d.multipliers;
   const float* __restrict__ gap = d.gaps;
   const std::uint32_t* __restrict__ offsets = d.incidence.offsets;
@@ -99,7 +99,10 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float load = 0.0f;
     const std::uint32_t begin = offsets[b];
-    const std::uint32_t end = offsets[b + 1];
+    std::uint32_t end = offsets[b + 1];
+    if (!index_ok(end, std::uint64_t(2) * d.row_count + 1, check) || !index_ok(begin, std::uint64_t(end) + 1, check)) {
+      end = begin;  // offsets out of range or not monotone: no entries
+    }
     for (std::uint32_t k0 = begin; k0 < end; k0 += kBatch) {
       float4 ea[kBatch], eb[kBatch];
       float gv[kBatch], pv[kBatch];
@@ -114,8 +117,9 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
           const std::uint32_t row = __float_as_uint(eb[t].w);
-          gv[t] = shared_load<Coherent>(&g[row]);
-          pv[t] = mode == 1 ? shared_load<Coherent>(&gap[row]) : 0.0f;
+          const bool ok = index_ok(row, d.row_count, check);
+          gv[t] = ok ? shared_load<Coherent>(&g[row]) : 0.0f;
+          pv[t] = ok && mode == 1 ? shared_load<Coherent>(&gap[row]) : 0.0f;
         }
       }
 #pragma unroll
@@ -146,7 +150,7 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_
   const SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
   if (fixed_mode < 0 && mode == 1 && d.proceed == 0u) return;  // an unrolled pair after convergence
-  body_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
+  body_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x, &desc->check_status);
 }
 
 // The row pass over rows block, block + blocks, ... of the grid; unless
@@ -154,7 +158,7 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_BODY_MIN_BLOCKS) body_pass_
 // d.partials[5 * block ...], reduced in a fixed tree.
 template <bool Coherent>
 __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
-                                         std::uint32_t blocks) {
+                                         std::uint32_t blocks, std::uint32_t* check) {
   const float dt = d.dt;
   float* __restrict__ g = d.multipliers;
   float* __restrict__ gap = d.gaps;
@@ -168,6 +172,7 @@ __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode,
     const float gi = shared_load<Coherent>(&g[i]);
     const float gpi = project ? shared_load<Coherent>(&gap[i]) : 0.0f;
     const uint2 s = __ldcs(&d.rows.slots[i]);
+    if (!index_ok(s.x, d.body_count, check) || (s.y != kInvalidSlot && !index_ok(s.y, d.body_count, check))) continue;
     const float4 ra = __ldcs(&d.rows.a[i]);
     const float4 rb = __ldcs(&d.rows.b[i]);
     const float4 rd = __ldcs(&d.rows.d[i]);
@@ -306,7 +311,7 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_ROW_MIN_BLOCKS) row_pass_ke
   SolveDesc& d = *desc;
   const std::uint32_t mode = fixed_mode >= 0 ? std::uint32_t(fixed_mode) : d.mode;
   if (fixed_mode < 0 && mode == 1 && d.proceed == 0u) return;  // an unrolled pair after convergence
-  row_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x);
+  row_pass<false>(d, mode, d.step, blockIdx.x, gridDim.x, &desc->check_status);
   if (mode == 2) return;
   __threadfence();
   __shared__ bool last;
@@ -399,9 +404,9 @@ __global__ void __launch_bounds__(kSolveThreads, MSB_RELAX_MIN_BLOCKS)
   std::uint32_t mode = 0;
   float alpha = 0.0f;
   for (;;) {
-    body_pass<true>(problem, mode, alpha, blockIdx.x, blocks);
+    body_pass<true>(problem, mode, alpha, blockIdx.x, blocks, &state->check_status);
     if (!grid_barrier(*state, blocks, -1)) return;
-    row_pass<true>(problem, mode, alpha, blockIdx.x, blocks);
+    row_pass<true>(problem, mode, alpha, blockIdx.x, blocks, &state->check_status);
     if (!grid_barrier(*state, blocks, int(mode))) return;
     if (shared->proceed == 0u) return;
     mode = 1;
@@ -434,6 +439,7 @@ __global__ void solve_reset_kernel(SolveDesc* desc) {
     desc->bound_bits = 0;
     desc->status = MSB_SOLVE_CONVERGED;
     desc->proceed = 0;
+    desc->check_status = 0;
   }
 }
 
@@ -458,10 +464,12 @@ __global__ void incidence_keys_kernel(const uint2* __restrict__ slots, std::uint
 }
 
 __global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __restrict__ values, std::uint32_t entries,
-                                        float4* __restrict__ out_a, float4* __restrict__ out_b) {
+                                        float4* __restrict__ out_a, float4* __restrict__ out_b,
+                                        std::uint32_t* status) {
   for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < entries; k += gridDim.x * blockDim.x) {
     const std::uint32_t v = values[k];
     const std::uint32_t row = v >> 1;
+    if (!index_ok(row, entries / 2, status)) continue;
     if (v & 1u) {
       const float4 c = r.c[row];
       const float4 d = r.d[row];
@@ -498,7 +506,7 @@ namespace {
 
 void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
                     std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
-                    cudaStream_t stream) {
+                    cudaStream_t stream, std::uint32_t* status) {
   cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
   if (row_count > 0) {
     incidence_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, body_count, keys,
@@ -512,7 +520,7 @@ void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_
   // A constraint row has no second entry; its key sorts past every body and
   // the offsets end before it, so gathering all 2R entries is harmless.
   incidence_gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(rows, values, std::uint32_t(n), incidence.a,
-                                                                 incidence.b);
+                                                                 incidence.b, status);
   count_launch();
 }
 
@@ -520,8 +528,8 @@ void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_
 
 void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
                      std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
-                     cudaStream_t stream) {
-  incidence_pass(rows, row_count, body_count, incidence, keys, values, counts, temp, stream);
+                     cudaStream_t stream, std::uint32_t* status) {
+  incidence_pass(rows, row_count, body_count, incidence, keys, values, counts, temp, stream, status);
 }
 
 void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,

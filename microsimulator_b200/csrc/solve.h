@@ -83,6 +83,7 @@ struct SolveDesc {
   std::uint32_t barrier_count;
   std::uint32_t barrier_generation;
   std::uint32_t barrier_abort;  // a barrier wait ran out of time: every block stops
+  std::uint32_t check_status;   // checked build: the first index check that failed (0: none)
 };
 
 // Builds the incidence of `rows` over `bodies` bodies.  Scratch: `keys` and
@@ -90,7 +91,7 @@ struct SolveDesc {
 // sort_temp_words(2 * rows) words.
 void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
                      std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
-                     cudaStream_t stream);
+                     cudaStream_t stream, std::uint32_t* status = nullptr);
 
 // Stable lists of each first slot's rows (ForceMemory's KeyedRows).
 void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,
