@@ -1041,7 +1041,7 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
   const SolveDesc& d = *c.host_desc;
   if (d.barrier_abort != 0) throw DeviceCheckError("a grid barrier of the relaxation ran out of time");
   if (d.check_status != 0) throw DeviceCheckError("an index check of the relaxation failed");
-  if (!fused) count_launch(int(2 * d.iterations));
+  if (!fused) count_launch(SolveGraph::loop_launches(d.iterations));
   c.solve_log.push_back({rows, d.iterations, d.status, d.residual});
   if (d.status == 3) throw std::invalid_argument("contact system has no positive diagonal");
   return {d.status, d.iterations, d.residual};

@@ -614,6 +614,11 @@ int SolveGraph::create(SolveDesc* desc, int blocks, cudaStream_t stream) {
   return err;
 }
 
+int SolveGraph::loop_launches(std::uint32_t iterations) {
+  const std::uint32_t evaluations = (iterations + MSB_WHILE_UNROLL - 1) / MSB_WHILE_UNROLL;
+  return int(evaluations * 2 * MSB_WHILE_UNROLL);
+}
+
 int SolveGraph::launch(cudaStream_t stream) {
   // Each graph has its own WHILE-node handle; the row pass reads it here.
   cudaError_t err = cudaMemcpyAsync(&desc_->handle, &handle_, sizeof(handle_), cudaMemcpyHostToDevice, stream);

@@ -110,6 +110,9 @@ class SolveGraph {
   int create(SolveDesc* desc, int blocks, cudaStream_t stream);
   int launch(cudaStream_t stream);
   int blocks() const { return blocks_; }
+  // Kernel launches of the WHILE node for a solve of `iterations`
+  // iterations (whole evaluations of its unrolled body).
+  static int loop_launches(std::uint32_t iterations);
 
  private:
   cudaGraph_t graph_ = nullptr;
