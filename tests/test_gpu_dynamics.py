@@ -331,3 +331,53 @@ def test_growing_colony_trajectory(backend, reference):
         assert len(gpu) > 50  # it grew and divided
     finally:
         reference.world_destroy(handle)
+
+
+def lockstep(backend, reference, world, walls, steps, p, seed, tolerance=2.0e-3):
+    """Steps `world` on the backend and on the reference CPU backend side by
+    side, every cell of length >= 4 divided before each step (daughter turns
+    +-0.02 rad, the plan taken from the reference's state); returns the
+    largest geometry difference seen and asserts it within `tolerance`
+    (absolute plus relative) after every step."""
+    handle = reference.world_create(world, walls)
+    worst = 0.0
+    try:
+        gpu, mirror = world.copy(), world.copy()
+        for step in range(steps):
+            plan = workloads.plan_divisions(mirror, 1.0, seed=seed + step, minimum_length=4.0)
+            for w in (gpu, mirror):
+                w.divide_many(plan.parents, 0.5, plan.rotations)
+            reference.world_divide(handle, plan.parents, plan.rotations)
+            backend.advance_contact_dynamics(gpu, walls, 0.02, p)
+            reference.world_step(handle, 0.02, p)
+            reference.world_read(handle, mirror)
+            gpu.next_id = mirror.next_id = int(mirror.ids.max()) + 1
+            assert np.array_equal(gpu.ids, mirror.ids)
+            worst = max(worst, float(np.max(np.abs(gpu.geometry() - mirror.geometry()))))
+            assert within(gpu.geometry(), mirror.geometry(), tolerance), (step, worst)
+        return worst, len(gpu)
+    finally:
+        reference.world_destroy(handle)
+
+
+@pytest.mark.parametrize("law", [GrowthLoadResponse(GrowthLoadLaw.EXPONENTIAL, sensitivity=2.0),
+                                 GrowthLoadResponse(GrowthLoadLaw.LINEAR, free_load=0.05, stall_load=0.5)])
+def test_load_sensitive_colony_in_lockstep(backend, reference, law):
+    """A colony whose growth falls with axial load (the reference's
+    load-sensitive colony, python/tests/test_contact_dynamics.py:450-…, and
+    the growth-load laws of contact_dynamics.cpp:600-612), stepped in lockstep
+    with the reference for 20 steps."""
+    world = workloads.colony_1k(seed=31, n=60, side=12.0, growth_rate=0.5)
+    p = ContactDynamicsParameters(overlap_tolerance=2.0e-4, growth=law)
+    worst, cells = lockstep(backend, reference, world, None, 20, p, seed=700)
+    assert cells > 62
+
+
+def test_trap_colony_with_walls_in_lockstep(backend, reference):
+    """Configuration 2's shape at small size: capsules in the trap with the
+    trap-channel device's wall boxes, growing and dividing for 12 steps in
+    lockstep with the reference."""
+    world, walls = workloads.trap_colony(n=400, seed=12, area_fraction=0.6)
+    p = ContactDynamicsParameters(overlap_tolerance=2.0e-4)
+    worst, cells = lockstep(backend, reference, world, walls, 12, p, seed=900)
+    assert cells > 400
