@@ -318,6 +318,17 @@ int msb_build_external_contact_graph(msb_context* context, const msb_external_co
                                      uint64_t cell_count, uint32_t device_pointers, uint64_t* incidence_offsets,
                                      uint64_t* incidence_contacts);
 
+/* ComputeBackend::find_external_contacts returning its whole
+ * ExternalContactGraph (backend.hpp:37-39, cpu_constraints.cpp:597): the
+ * contacts of msb_find_external_contacts and, from the same device-resident
+ * list, the incidence of msb_build_external_contact_graph (host arrays:
+ * cells->count + 1 offsets and one index per contact; null offsets: none). */
+int msb_find_external_contact_graph(msb_context* context, const msb_cell_arrays* cells,
+                                    const msb_constraint* constraints, uint64_t constraint_count,
+                                    const msb_constraint_contact_parameters* parameters, uint32_t every_face,
+                                    msb_external_contact* contacts, uint64_t capacity, uint64_t* count,
+                                    uint64_t* incidence_offsets, uint64_t* incidence_contacts);
+
 /* ComputeBackend::find_cell_contacts returning its whole ContactGraph
  * (backend.hpp:35-36, cpu_contacts.cpp:211): the contacts of
  * msb_find_cell_contacts and, from the same device-resident list, the index

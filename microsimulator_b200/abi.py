@@ -350,6 +350,11 @@ SIGNATURES = {
          c_void_p],
     ),
     "msb_build_contact_graph": (c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_void_p]),
+    "msb_find_external_contact_graph": (
+        c_int,
+        [c_void_p, POINTER(CellArrays), c_void_p, c_uint64, POINTER(ConstraintContactParameters), c_uint32,
+         c_void_p, c_uint64, POINTER(c_uint64), c_void_p, c_void_p],
+    ),
     "msb_build_external_contact_graph": (
         c_int, [c_void_p, c_void_p, c_uint64, c_uint64, c_uint32, c_void_p, c_void_p]),
     "msb_find_external_contacts": (

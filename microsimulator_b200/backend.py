@@ -207,6 +207,33 @@ class B200Backend:
                                                       cell_count, 0, ctypes.byref(index)))
         return self._graph(cell_count, records.copy(), index, arrays)
 
+    def find_external_contact_graph(self, world, constraints,
+                                    parameters: ConstraintContactParameters | None = None,
+                                    every_face: bool = False) -> ExternalContactGraph:
+        """find_external_contacts returning its whole ExternalContactGraph:
+        the contacts and their incidence, built on the device from the
+        contacts as found."""
+        parameters = parameters or ConstraintContactParameters()
+        cells = world.arrays()
+        native = parameters.native()
+        n = len(world)
+        capacity = max(self._capacity, 4 * n + 16)
+        while True:
+            contacts = np.zeros(capacity, dtype=abi.EXTERNAL_CONTACT_DTYPE)
+            offsets = np.zeros(n + 1, dtype=np.uint64)
+            indices = np.zeros(capacity, dtype=np.uint64)
+            count = c_uint64(0)
+            status = self._lib.msb_find_external_contact_graph(
+                self._handle, ctypes.byref(cells), c_void_p(constraints.pointer()), len(constraints),
+                ctypes.byref(native), 1 if every_face else 0, c_void_p(abi.ptr(contacts)), capacity,
+                ctypes.byref(count), c_void_p(abi.ptr(offsets)), c_void_p(abi.ptr(indices)))
+            if status == abi.ERR_CAPACITY and count.value > capacity:
+                capacity = int(count.value) + 16
+                continue
+            self._check(status)
+            total = int(count.value)
+            return ExternalContactGraph(n, contacts[:total].copy(), offsets, indices[:total].copy())
+
     def build_contact_graph_device(self, contacts_pointer: int, count: int, cell_count: int, index) -> int:
         """msb_build_contact_graph on device-resident contact records and
         index arrays (``graph.device_index``); returns the packed neighbour

@@ -773,6 +773,45 @@ void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
   read_scalars(c);
 }
 
+// A constraint record as ConstraintSet holds it: the checks of
+// validate_plane / _sphere / _box / _cylinder (cpp/core/constraints.cpp:17-80),
+// which a set built by add_plane etc. meets (a plane's inward normal is
+// stored normalized, constraints.cpp:169-186).
+void validate_constraint(const msb_constraint& k) {
+  const auto finite3 = [](const msb_vec3& v) { return std::isfinite(v.x) && std::isfinite(v.y) && std::isfinite(v.z); };
+  if (!std::isfinite(k.coefficient) || k.coefficient <= 0.0f) {
+    throw std::invalid_argument("constraint coefficient must be finite and positive");
+  }
+  const bool region_ok = k.allowed_region == MSB_REGION_OUTSIDE || k.allowed_region == MSB_REGION_INSIDE;
+  switch (k.kind) {
+    case MSB_CONSTRAINT_PLANE: {
+      if (!finite3(k.a) || !finite3(k.b)) throw std::invalid_argument("plane contains an invalid field");
+      // norm() of types.hpp in FP32: sqrt((x*x + y*y) + z*z).
+      const float length = std::sqrt((k.b.x * k.b.x + k.b.y * k.b.y) + k.b.z * k.b.z);
+      if (std::fabs(length - 1.0f) > 1.0e-5f) throw std::invalid_argument("plane inward normal is not normalized");
+      return;
+    }
+    case MSB_CONSTRAINT_SPHERE:
+      if (!finite3(k.a) || !std::isfinite(k.radius) || k.radius <= 0.0f) {
+        throw std::invalid_argument("sphere contains invalid geometry");
+      }
+      break;
+    case MSB_CONSTRAINT_BOX:
+      if (!finite3(k.a) || !std::isfinite(k.b.x) || !(k.b.x > 0.0f) || !std::isfinite(k.b.y) || !(k.b.y > 0.0f) ||
+          !std::isfinite(k.b.z) || !(k.b.z > 0.0f)) {
+        throw std::invalid_argument("box contains invalid geometry");
+      }
+      break;
+    default:
+      if (!finite3(k.a) || !std::isfinite(k.radius) || k.radius <= 0.0f || !std::isfinite(k.half_height) ||
+          k.half_height <= 0.0f) {
+        throw std::invalid_argument("cylinder contains invalid geometry");
+      }
+      break;
+  }
+  if (!region_ok) throw std::invalid_argument("constraint uses an unknown allowed region");
+}
+
 void load_constraints(Ctx& c, const msb_constraint* constraints, std::uint64_t count) {
   if (count > 0 && constraints == nullptr) throw std::invalid_argument("constraint array must not be null");
   std::vector<DeviceConstraint> sorted(count);
@@ -780,6 +819,7 @@ void load_constraints(Ctx& c, const msb_constraint* constraints, std::uint64_t c
     const auto& k = constraints[i];
     if (k.kind > MSB_CONSTRAINT_CYLINDER) throw std::invalid_argument("constraint kind is invalid");
     if (k.id == 0) throw std::invalid_argument("constraint identifier is invalid");
+    validate_constraint(k);
     static_assert(sizeof(DeviceConstraint) == sizeof(msb_constraint));
     std::memcpy(&sorted[i], &k, sizeof(k));
   }
@@ -2065,6 +2105,43 @@ int msb_find_cell_contact_graph(msb_context* context, const msb_cell_arrays* cel
     }
     if (total > 0) {
       check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_cell_contact), cudaMemcpyDeviceToHost,
+                            c.stream),
+            "copy contacts");
+    }
+    sync(c);
+  });
+}
+
+int msb_find_external_contact_graph(msb_context* context, const msb_cell_arrays* cells,
+                                    const msb_constraint* constraints, uint64_t constraint_count,
+                                    const msb_constraint_contact_parameters* parameters, uint32_t every_face,
+                                    msb_external_contact* contacts, uint64_t capacity, uint64_t* count,
+                                    uint64_t* incidence_offsets, uint64_t* incidence_contacts) {
+  return guarded(context, [&] {
+    if (cells == nullptr || parameters == nullptr || count == nullptr) throw std::invalid_argument("null argument");
+    validate_constraint_parameters(*parameters);
+    auto& c = *context;
+    load_cells(c, *cells, false);
+    load_constraints(c, constraints, constraint_count);
+    const std::uint32_t total =
+        find_walls(c, c.state, parameters->activation_margin, parameters->degeneracy_epsilon, every_face != 0,
+                   c.touches, 0);
+    *count = total;
+    if (total > capacity) throw CapacityError("contact array is too small");
+    if (total > 0 && contacts == nullptr) throw std::invalid_argument("null contact array");
+    if (incidence_offsets != nullptr && total > 0 && incidence_contacts == nullptr) {
+      throw std::invalid_argument("null incidence array");
+    }
+    c.records.ensure(std::max<std::uint64_t>(total, 1) * sizeof(msb_external_contact));
+    if (total > 0) launch_touches_to_external_contacts(c.touches.p, total, c.ids.p, c.records.p, c.stream);
+    if (incidence_offsets != nullptr) {
+      const GraphArrays g = graph_staging(c, cells->count, total, false);
+      build_graph(c, c.records.p, total, cells->count, true, g);
+      copy_out(c, incidence_offsets, g.incidence_offsets, (cells->count + 1) * 8);
+      copy_out(c, incidence_contacts, g.incidence, std::uint64_t(total) * 8);
+    }
+    if (total > 0) {
+      check(cudaMemcpyAsync(contacts, c.records.p, total * sizeof(msb_external_contact), cudaMemcpyDeviceToHost,
                             c.stream),
             "copy contacts");
     }

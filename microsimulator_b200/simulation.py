@@ -100,8 +100,7 @@ class Simulation:
     def find_external_contacts(self, parameters: ConstraintContactParameters | None = None) -> ExternalContactGraph:
         """Simulation::find_external_contacts: the ExternalContactGraph of the
         cells against the constraints."""
-        contacts = self.backend.find_external_contacts(self.world, self.constraints, parameters, every_face=False)
-        return self.backend.build_external_contact_graph(contacts, len(self.world))
+        return self.backend.find_external_contact_graph(self.world, self.constraints, parameters)
 
     def solve_contact_system(self, system: ContactSystem, initial_multipliers,
                              parameters: ContactSolveParameters | None = None) -> ContactSolveResult:

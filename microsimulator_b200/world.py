@@ -294,18 +294,51 @@ class ConstraintSet:
         self.next_id += 1
         return self.next_id - 1
 
+    @staticmethod
+    def _finite(*values) -> bool:
+        return all(np.isfinite(f32(v)) for v in values)
+
+    @staticmethod
+    def _check_coefficient(coefficient) -> None:
+        if not np.isfinite(f32(coefficient)) or f32(coefficient) <= 0:
+            raise ValueError("constraint coefficient must be finite and positive")
+
     def add_plane(self, point=(0.0, 0.0, 0.0), inward_normal=(0.0, 1.0, 0.0), coefficient=1.0) -> int:
-        return self._add(abi.CONSTRAINT_PLANE, abi.REGION_OUTSIDE, point, inward_normal, coefficient=coefficient)
+        """ConstraintSet::add_plane (constraints.cpp:169-186): the inward
+        normal is stored normalized, inward_normal * (1 / |inward_normal|) in
+        FP32."""
+        if not self._finite(*point, *inward_normal):
+            raise ValueError("plane fields must be finite")
+        x, y, z = (f32(c) for c in inward_normal)
+        magnitude = np.sqrt(f32(f32(x * x) + f32(y * y)) + f32(z * z), dtype=f32)
+        if not np.isfinite(magnitude) or magnitude <= 0:
+            raise ValueError("plane inward normal must be non-zero")
+        self._check_coefficient(coefficient)
+        scale = f32(f32(1.0) / magnitude)
+        normal = (f32(x * scale), f32(y * scale), f32(z * scale))
+        return self._add(abi.CONSTRAINT_PLANE, abi.REGION_OUTSIDE, point, normal, coefficient=coefficient)
 
     def add_sphere(self, center=(0.0, 0.0, 0.0), radius=1.0, coefficient=1.0, allowed_region=abi.REGION_OUTSIDE) -> int:
+        """ConstraintSet::add_sphere (constraints.cpp:188-201)."""
+        if not self._finite(*center, radius) or f32(radius) <= 0:
+            raise ValueError("sphere geometry must be finite with a positive radius")
+        self._check_coefficient(coefficient)
         return self._add(abi.CONSTRAINT_SPHERE, allowed_region, center, radius=radius, coefficient=coefficient)
 
     def add_box(self, center=(0.0, 0.0, 0.0), half_extents=(1.0, 1.0, 1.0), coefficient=1.0, allowed_region=abi.REGION_OUTSIDE) -> int:
+        """ConstraintSet::add_box (constraints.cpp:203-216)."""
+        if not self._finite(*center, *half_extents) or any(f32(h) <= 0 for h in half_extents):
+            raise ValueError("box geometry must be finite with positive half extents")
+        self._check_coefficient(coefficient)
         return self._add(abi.CONSTRAINT_BOX, allowed_region, center, half_extents, coefficient=coefficient)
 
     def add_cylinder(
         self, center=(0.0, 0.0, 0.0), radius=1.0, half_height=1.0, coefficient=1.0, allowed_region=abi.REGION_OUTSIDE
     ) -> int:
+        """ConstraintSet::add_cylinder (constraints.cpp:218-234)."""
+        if not self._finite(*center, radius, half_height) or f32(radius) <= 0 or f32(half_height) <= 0:
+            raise ValueError("cylinder geometry must be finite with a positive radius and half height")
+        self._check_coefficient(coefficient)
         return self._add(
             abi.CONSTRAINT_CYLINDER, allowed_region, center, radius=radius, half_height=half_height, coefficient=coefficient
         )

@@ -7,7 +7,7 @@ import pytest
 
 from microsimulator_b200 import abi, workloads
 from microsimulator_b200.types import ConstraintContactParameters, ContactParameters
-from microsimulator_b200.world import WorldState
+from microsimulator_b200.world import ConstraintSet, WorldState
 from tests.golden.make_golden import wall_set, world_from
 
 pytestmark = pytest.mark.gpu
@@ -123,3 +123,21 @@ def test_invalid_inputs_raise(backend):
     w.position_x[0] = np.nan
     with pytest.raises(ValueError):
         backend.find_cell_contacts(w)
+
+
+@pytest.mark.parametrize("field,value", [("b", (0.0, 2.0, 0.0)), ("coefficient", 0.0), ("radius", -1.0),
+                                         ("allowed_region", 7)])
+def test_invalid_constraint_records_raise(backend, field, value):
+    """Constraint records meet ConstraintSet's checks (constraints.cpp:17-80):
+    a plane's inward normal normalized, a positive coefficient, positive
+    radii, a known region.  A record that does not is an error, not a
+    silently different wall."""
+    w = WorldState()
+    w.add_cell((0, 0.25, 0), (1, 0, 0), 2.0, 0.5)
+    cs = ConstraintSet()
+    cs.add_plane(point=(0.0, 0.0, 0.0), inward_normal=(0.0, 1.0, 0.0))
+    cs.add_sphere(center=(5.0, 0.0, 0.0), radius=1.0)
+    target = 1 if field == "radius" or field == "allowed_region" else 0
+    cs.records[target][field] = value
+    with pytest.raises(ValueError):
+        backend.find_external_contacts(w, cs)

@@ -196,3 +196,35 @@ def test_slot_index_space_and_empty_graphs(backend):
     assert status == abi.ERR_OVERFLOW
     external = np.zeros(0, dtype=abi.EXTERNAL_CONTACT_DTYPE)
     assert backend.build_external_contact_graph(external, 3).incidence_offsets.tolist() == [0, 0, 0, 0]
+
+
+def test_plane_constraint_graph_through_the_simulation_api(backend):
+    """The reference's test_plane_constraint_graph_is_typed_and_incident
+    (python/tests/test_simulation.py:323-357), on this backend."""
+    sim = Simulation(backend=backend)
+    cell_id = sim.add_cell(position=(0.0, 0.25, 0.0), length=2.0, radius=0.5)
+    constraint_id = sim.add_plane_constraint(point=(0.0, 0.0, 0.0), inward_normal=(0.0, 2.0, 0.0), coefficient=3.0)
+    graph = sim.find_external_contacts()
+    assert graph.cell_count == 1
+    assert len(graph) == 2
+    assert graph.incident_contact_indices(0) == [0, 1]
+    assert np.all(graph.contacts["cell_id"] == cell_id)
+    assert np.all(graph.contacts["constraint_id"] == constraint_id)
+    assert np.all(graph.contacts["constraint_kind"] == abi.CONSTRAINT_PLANE)
+    assert graph.contacts["location"].tolist() == [abi.ROD_NEGATIVE, abi.ROD_POSITIVE]
+    assert np.allclose(graph.contacts["signed_separation"], -0.25)
+    assert np.allclose(graph.contacts["normal"][:, 1], -1.0)
+    assert np.allclose(graph.contacts["point_on_cell"][:, 1], -0.25)
+    assert np.allclose(graph.contacts["weight"], 3.0 / np.sqrt(2.0), rtol=1e-6)
+
+
+def test_found_external_graph_is_the_references(backend, golden):
+    from tests.golden.make_golden import wall_set, world_from
+    from microsimulator_b200.types import ConstraintContactParameters
+
+    data = golden("contact_graph")
+    world = world_from(golden("colony_1k"), "world__")
+    graph = backend.find_external_contact_graph(world, wall_set(), ConstraintContactParameters(0.1), every_face=True)
+    assert graph.contacts.tobytes() == golden("walls")["walls_1_0.1"].tobytes()
+    assert np.array_equal(graph.incidence_offsets, data["walls__incidence_offsets"])
+    assert np.array_equal(graph.incidence_contacts, data["walls__incidence"])
