@@ -181,3 +181,63 @@ def test_drift_on_a_3d_lattice_is_the_references(backend, reference, solid):
     assert rg.report.substeps == rr.substeps
     assert np.max(np.abs(gpu.geometry()[:, 2] - world.geometry()[:, 2])) > 1e-5  # vertical drift too
     assert np.array_equal(gpu.geometry(), ref.geometry()), np.max(np.abs(gpu.geometry() - ref.geometry()))
+
+
+def line_field(origin, spacing, sites, speed, obstacles=None, x_faces=None):
+    """A line of sites along x (closed ends) carrying `speed` on its inner
+    faces, as the reference's uniform_flow_grid does on an open line."""
+    xf = np.zeros((sites + 1, 1, 1), np.float32)
+    if x_faces is None:
+        xf[1:sites, 0, 0] = speed
+    else:
+        xf[:, 0, 0] = x_faces
+    yf = np.zeros((sites, 2, 1), np.float32)
+    zf = np.zeros((sites, 1, 2), np.float32)
+    mask = None if obstacles is None else np.asarray(obstacles, np.uint8).reshape(sites, 1, 1)
+    return FlowField((sites, 1, 1), (origin, 0.0, 0.0), (spacing, 1.0, 1.0), xf, yf, zf, mask)
+
+
+@pytest.mark.parametrize(("origin", "spacing"), [(0.0, 1.0), (0.1, 0.3), (-97.5, 1.65), (0.7, 5.0)])
+def test_drift_clamps_at_the_lattice_ends_as_the_reference(backend, reference, origin, spacing):
+    """The clamped stencil at and beyond the last site (the reference's
+    test_flow_drift_clamps_endpoints_on_any_lattice, test_simulation.py:500-524),
+    inside the step: bit-exact against the reference's step."""
+    sites = 33
+    world = WorldState()
+    world.add_cell(position=(origin + spacing * (sites - 1), 0.0, 0.0), direction=(1.0, 0.0, 0.0),
+                   length=2.0 * spacing, radius=0.3, growth_rate=0.0)
+    world.add_cell(position=(origin + spacing * (sites + 3), 4.0, 0.0), direction=(0.0, 1.0, 0.0),
+                   length=2.0 * spacing, radius=0.3, growth_rate=0.0)  # beyond the lattice
+    world.add_cell(position=(origin + spacing * 7.3, -3.0, 0.0), direction=(0.6, 0.8, 0.0),
+                   length=2.0 * spacing, radius=0.3, growth_rate=0.0)
+    f = line_field(origin, spacing, sites, 2.0)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        rg = backend.advance_contact_dynamics(gpu, None, 0.1, p)
+    finally:
+        backend.set_flow_field(None)
+    rr = reference.flow_step(ref, f, 0.1, p)
+    assert rg.report.substeps == rr.substeps
+    assert np.array_equal(gpu.geometry(), ref.geometry()), np.max(np.abs(gpu.geometry() - ref.geometry()))
+    assert gpu.position_x[2] > world.position_x[2]  # an interior cell moved with the flow
+
+
+def test_a_buried_cell_samples_no_flow(backend, reference):
+    """A cell pressed into a solid site samples no flow and does not move
+    (the reference's test_a_cell_inside_a_wall_samples_no_flow_and_does_not_drift,
+    test_simulation.py:569-598), inside the step, bit-exact."""
+    f = line_field(0.0, 1.0, 5, 2.0, obstacles=[0, 0, 1, 0, 0], x_faces=[0.0, 2.0, 0.0, 0.0, 2.0, 0.0])
+    world = WorldState()
+    world.add_cell(position=(2.0, 0.0, 0.0), direction=(1.0, 0.0, 0.0), length=0.0, radius=0.3, growth_rate=0.0)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4, flow_drift=True)
+    gpu, ref = world.copy(), world.copy()
+    backend.set_flow_field(f)
+    try:
+        backend.advance_contact_dynamics(gpu, None, 0.5, p)
+    finally:
+        backend.set_flow_field(None)
+    reference.flow_step(ref, f, 0.5, p)
+    assert gpu.position_x[0] == 2.0
+    assert np.array_equal(gpu.geometry(), ref.geometry())
