@@ -2397,7 +2397,8 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     load_constraints(c, constraints, constraint_count);
     c.has_memory = c.has_memory && (c.warm_start_mode & kWarmCarry) != 0;
     if (dynamics->flow_drift != 0 && !c.has_flow) {
-      throw std::invalid_argument("flow drift requires a flow field (msb_set_flow_field)");
+      // Simulation::step's error (simulation.cpp:194), a logic_error: MSB_ERR_RUNTIME.
+      throw std::logic_error("flow drift requires a signal grid with a velocity field (msb_set_flow_field)");
     }
     if (c.has_guess && c.guess_cells != c.n) {
       c.has_guess = false;

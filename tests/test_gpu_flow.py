@@ -116,7 +116,9 @@ def test_flow_drift_needs_a_field(backend):
     world = colony(n=20)
     p = ContactDynamicsParameters(flow_drift=True)
     before = world.copy()
-    with pytest.raises(ValueError):
+    # Simulation::step throws logic_error (simulation.cpp:194), which the
+    # reference's bindings raise as RuntimeError.
+    with pytest.raises(RuntimeError, match="velocity field"):
         backend.advance_contact_dynamics(world, None, DT, p)
     assert np.array_equal(before.geometry(), world.geometry())
     with pytest.raises(ValueError):
@@ -241,3 +243,37 @@ def test_a_buried_cell_samples_no_flow(backend, reference):
     reference.flow_step(ref, f, 0.5, p)
     assert gpu.position_x[0] == 2.0
     assert np.array_equal(gpu.geometry(), ref.geometry())
+
+
+def test_flow_carries_cells_inside_the_solve(backend):
+    """The reference's test_flow_carries_cells_inside_the_solve
+    (python/tests/test_contact_dynamics.py:576-631): a uniform flow of 0.5 on a
+    line of 9 sites carries a free cell at its own speed until a fixed cell
+    downstream stops it at contact."""
+    from microsimulator_b200.simulation import Simulation
+
+    sim = Simulation(backend=backend)
+    sites = 9
+    xf = np.full((sites + 1, 1, 1), 0.5, np.float32)
+    f = FlowField((sites, 1, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), xf, np.zeros((sites, 2, 1), np.float32),
+                  np.zeros((sites, 1, 2), np.float32), None)
+    free = sim.add_cell(position=(2.0, 0.0, 0.0), length=1.0, radius=0.25, growth_rate=0.0)
+    fixed = sim.add_cell(position=(3.6, 0.0, 0.0), length=1.0, radius=0.25, growth_rate=0.0, fixed=True)
+    p = ContactDynamicsParameters(flow_drift=True)
+    backend.set_flow_field(f)
+    try:
+        result = sim.step(0.1, p)
+        assert abs(sim.cell(free)["position"][0] - 2.05) <= 1e-5
+        assert result.center_velocities[sim.cell(free)["slot"]][0] == pytest.approx(0.5)
+        assert result.center_velocities[sim.cell(fixed)["slot"]][0] == 0.0
+        for _ in range(9):
+            result = sim.step(0.1, p)
+        stopped = sim.cell(free)["position"][0]
+        assert 2.1 - 2e-3 <= stopped <= 2.1 + 2e-3
+        assert abs(result.center_velocities[sim.cell(free)["slot"]][0]) < 2e-3
+        assert result.report.max_overlap < 2e-3
+        assert abs(sim.cell(fixed)["position"][0] - 3.6) <= 1e-6
+        sim.step(0.1, ContactDynamicsParameters())
+        assert abs(sim.cell(free)["position"][0] - stopped) <= 2e-3
+    finally:
+        backend.set_flow_field(None)

@@ -74,3 +74,40 @@ def test_finite_wall_detects_midspan_capsule_contact(sim):
     assert math.isclose(contact["signed_separation"], -0.75, abs_tol=2.0e-5)
     sim.step(0.05, ContactDynamicsParameters())
     assert sim.cell(cell_id)["position"][1] > 0.75
+
+
+def spanning_pair(backend, tilt):
+    """_spanning_pair of test_contact_dynamics.py:534-548: two cells end to
+    end that exactly span a closed 4 by 4 chamber."""
+    sim = Simulation(backend=backend)
+    sim.add_box_constraint(half_extents=(2.0, 2.0, 0.6), allowed_region=abi.REGION_INSIDE)
+    for sign in (-1.0, 1.0):
+        sim.add_cell(position=(sign * 1.0, 0.0, 0.0), direction=(math.cos(sign * tilt), math.sin(sign * tilt), 0.0),
+                     length=1.2, radius=0.4)
+    return sim
+
+
+def test_collinear_cells_spanning_a_chamber_buckle(backend):
+    """test_contact_dynamics.py:551-573: growth that ignores load turns the
+    pair out of line; a perfectly straight pair with a load response stalls."""
+    from microsimulator_b200.types import GrowthLoadLaw, GrowthLoadResponse
+
+    sim = spanning_pair(backend, 0.01)
+    parameters = ContactDynamicsParameters()
+    result = sim.step(0.0, parameters)
+    for _ in range(12):
+        result = sim.step(0.05, parameters)
+    w = sim.world
+    assert np.all(np.abs(w.direction_y) > 0.3)
+    assert np.all(w.lengths > 1.2 * 1.6)
+    assert result.report.max_overlap < 0.01
+    assert np.all(np.abs(w.position_z) < 1e-3)
+
+    straight = spanning_pair(backend, 0.0)
+    stalling = ContactDynamicsParameters(growth=GrowthLoadResponse(GrowthLoadLaw.LINEAR, stall_load=4.0))
+    stalling.wall_stiffness = stalling.contact_stiffness
+    for _ in range(40):
+        straight.step(0.05, stalling)
+    w = straight.world
+    assert np.all(w.direction_y == 0.0)
+    assert np.all(np.abs(w.lengths - 1.2) <= 5e-3)
