@@ -141,3 +141,26 @@ def test_invalid_constraint_records_raise(backend, field, value):
     cs.records[target][field] = value
     with pytest.raises(ValueError):
         backend.find_external_contacts(w, cs)
+
+
+def test_constraint_conformance_fixtures(backend, reference):
+    """The reference's constraint conformance test
+    (tests/conformance/constraint_conformance_test.cpp:155-240): every fixture's
+    ExternalContactGraph equal to the reference's (its contacts bit for bit,
+    its incidence exactly), and the empty inputs."""
+    from tests.constraint_fixtures import FIXTURES
+
+    for name, build in FIXTURES.items():
+        world, constraints = build()
+        expected = reference.find_external_contacts(world, constraints)
+        offsets, indices = reference.external_contact_graph(expected, len(world))
+        graph = backend.find_external_contact_graph(world, constraints)
+        assert graph.contacts.tobytes() == expected.tobytes(), name
+        assert np.array_equal(graph.incidence_offsets, offsets), name
+        assert np.array_equal(graph.incidence_contacts, indices), name
+    empty = backend.find_external_contact_graph(WorldState(), ConstraintSet())
+    assert empty.empty and empty.cell_count == 0
+    one = WorldState()
+    one.add_cell((0, 0, 0), (1, 0, 0), 1.0, 0.5)
+    graph = backend.find_external_contact_graph(one, ConstraintSet())
+    assert graph.empty and graph.cell_count == 1

@@ -194,3 +194,15 @@ def test_division_matches_reference_world(reference):
     local.divide_many(plan.parents, 0.5, plan.rotations)
     assert np.array_equal(local.ids, mirrored.ids)
     assert np.array_equal(local.geometry(), mirrored.geometry())
+
+
+def test_constraint_conformance_fixtures(oracle, reference):
+    """The reference's constraint conformance fixtures
+    (tests/conformance/constraint_conformance_test.cpp:19-153): the FP32
+    oracle's wall contacts equal the reference's, field for field."""
+    from tests.constraint_fixtures import FIXTURES
+
+    for name, build in FIXTURES.items():
+        world, constraints = build()
+        expected = reference.find_external_contacts(world, constraints)
+        assert oracle.find_external_contacts(world, constraints).tobytes() == expected.tobytes(), name
