@@ -228,3 +228,54 @@ def test_found_external_graph_is_the_references(backend, golden):
     assert graph.contacts.tobytes() == golden("walls")["walls_1_0.1"].tobytes()
     assert np.array_equal(graph.incidence_offsets, data["walls__incidence_offsets"])
     assert np.array_equal(graph.incidence_contacts, data["walls__incidence"])
+
+
+def reference_graph_equal(backend, reference, world, parameters=None):
+    """The backend's ContactGraph of `world` equals the reference CPU
+    backend's: contacts bit for bit, incidence exactly
+    (contact_conformance_test.cpp's compare_graphs at zero tolerance)."""
+    parameters = parameters or ContactParameters()
+    graph = backend.find_cell_contact_graph(world, parameters)
+    expected = reference.find_cell_contacts(world, parameters)
+    offsets, indices = reference.incidence(world, parameters)
+    assert graph.contacts.tobytes() == expected.tobytes()
+    assert np.array_equal(graph.incidence_offsets, offsets)
+    assert np.array_equal(graph.incidence_contacts, indices)
+    return graph
+
+
+def capsules(*specs):
+    from microsimulator_b200.world import WorldState
+
+    w = WorldState()
+    for center, axis, *length in specs:
+        w.add_cell(position=center, direction=axis, length=length[0] if length else 2.0, radius=0.5)
+    return w
+
+
+def test_contact_conformance_fixtures(backend, reference):
+    """The reference's contact conformance test
+    (tests/conformance/contact_conformance_test.cpp:55-160): mixed geometry,
+    31 coincident capsules (930 contacts, 60 incident on the first), margins
+    and buffer reuse, and the ids after a division."""
+    mixed = capsules(((0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 4.0), ((0.0, 0.8, 0.0), (-1.0, 0.0, 0.0), 4.0),
+                     ((4.9, 0.0, 0.0), (1.0, 0.0, 0.0), 4.0), ((10.0, 0.0, 0.0), (1.0, 0.0, 0.0)),
+                     ((10.0, 0.0, 0.0), (0.0, 1.0, 0.0)), ((15.0, 0.0, 0.0), (1.0, 0.0, 0.0), 0.0),
+                     ((15.0, 0.8, 0.0), (1.0, 0.0, 0.0), 0.0))
+    reference_graph_equal(backend, reference, mixed)
+
+    dense = capsules(*[((0.0, 0.0, 0.0), (1.0, 0.0, 0.0))] * 31)
+    graph = reference_graph_equal(backend, reference, dense)
+    assert len(graph) == 930
+    assert len(graph.incident_contact_indices(0)) == 60
+
+    reuse = capsules(((0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 0.0), ((1.005, 0.0, 0.0), (1.0, 0.0, 0.0), 0.0))
+    strict = reference_graph_equal(backend, reference, reuse, ContactParameters(activation_margin=0.0))
+    assert strict.empty
+    reference_graph_equal(backend, reference, reuse)
+    reuse.add_cell(position=(0.5, 0.0, 0.0), direction=(1.0, 0.0, 0.0), length=0.0, radius=0.5)
+    reference_graph_equal(backend, reference, reuse)
+
+    divided = capsules(((0.0, 0.0, 0.0), (1.0, 0.0, 0.0), 4.0), ((0.0, 0.2, 0.0), (1.0, 0.0, 0.0), 4.0))
+    divided.divide_many([int(divided.ids[0])], 0.5)
+    reference_graph_equal(backend, reference, divided)
