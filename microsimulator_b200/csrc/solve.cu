@@ -445,31 +445,115 @@ __global__ void solve_reset_kernel(SolveDesc* desc) {
 
 // ------------------------------------------------------------- incidence
 
-__global__ void incidence_keys_kernel(const uint2* __restrict__ slots, std::uint32_t rows, std::uint32_t bodies,
-                                      std::uint32_t* __restrict__ keys, std::uint32_t* __restrict__ values,
-                                      std::uint32_t* __restrict__ counts) {
+// Entries per body: one for a row's first slot, one for its second (a
+// constraint row has none).
+__global__ void incidence_counts_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
+                                        std::uint32_t* __restrict__ counts) {
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
     const uint2 s = slots[i];
-    keys[2 * std::uint64_t(i)] = s.x;
-    values[2 * std::uint64_t(i)] = i << 1;
     atomicAdd(&counts[s.x], 1u);
-    if (s.y != kInvalidSlot) {
-      keys[2 * std::uint64_t(i) + 1] = s.y;
-      atomicAdd(&counts[s.y], 1u);
-    } else {
-      keys[2 * std::uint64_t(i) + 1] = bodies;  // sorts past every body
-    }
-    values[2 * std::uint64_t(i) + 1] = (i << 1) | 1u;
+    if (s.y != kInvalidSlot) atomicAdd(&counts[s.y], 1u);
   }
 }
 
-__global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __restrict__ values, std::uint32_t entries,
+// Each entry (row << 1 | side) to a free place in its body's range, in any
+// order (the counts run back to zero).
+__global__ void incidence_scatter_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
+                                         const std::uint32_t* __restrict__ offsets,
+                                         std::uint32_t* __restrict__ counts, std::uint32_t* __restrict__ values) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const uint2 s = slots[i];
+    values[offsets[s.x] + atomicSub(&counts[s.x], 1u) - 1u] = i << 1;
+    if (s.y != kInvalidSlot) values[offsets[s.y] + atomicSub(&counts[s.y], 1u) - 1u] = (i << 1) | 1u;
+  }
+}
+
+template <int N>
+__device__ __forceinline__ void bitonic_sort_u32(std::uint32_t (&v)[N]) {
+#pragma unroll
+  for (int k = 2; k <= N; k <<= 1) {
+#pragma unroll
+    for (int j = k >> 1; j > 0; j >>= 1) {
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        const int l = i ^ j;
+        if (l > i) {
+          const std::uint32_t a = v[i], b = v[l];
+          const bool swap = (i & k) == 0 ? (a > b) : (a < b);
+          v[i] = swap ? b : a;
+          v[l] = swap ? a : b;
+        }
+      }
+    }
+  }
+}
+
+constexpr std::uint32_t kRegisterEntries = 16;
+constexpr std::uint32_t kLocalEntries = 64;
+
+__device__ __noinline__ void sort_local(std::uint32_t* __restrict__ values, std::uint32_t begin, std::uint32_t k) {
+  std::uint32_t v[kLocalEntries];
+  for (std::uint32_t j = 0; j < k; ++j) v[j] = values[begin + j];
+  for (std::uint32_t i = 1; i < k; ++i) {
+    const std::uint32_t x = v[i];
+    std::uint32_t j = i;
+    while (j > 0 && v[j - 1] > x) {
+      v[j] = v[j - 1];
+      --j;
+    }
+    v[j] = x;
+  }
+  for (std::uint32_t j = 0; j < k; ++j) values[begin + j] = v[j];
+}
+
+__device__ __noinline__ void sort_global(std::uint32_t* __restrict__ values, std::uint32_t begin, std::uint32_t k) {
+  for (std::uint32_t i = 1; i < k; ++i) {
+    const std::uint32_t x = values[begin + i];
+    std::uint32_t j = i;
+    while (j > 0 && values[begin + j - 1] > x) {
+      values[begin + j] = values[begin + j - 1];
+      --j;
+    }
+    values[begin + j] = x;
+  }
+}
+
+// One thread per body: its entries sorted by row (row << 1 | side orders as
+// the row), the order of make_incidence (cpp/cpu/cpu_contact_dynamics.cpp:78-106).
+__global__ void incidence_order_kernel(const std::uint32_t* __restrict__ offsets, std::uint32_t bodies,
+                                       std::uint32_t* __restrict__ values) {
+  for (std::uint32_t b = blockIdx.x * blockDim.x + threadIdx.x; b < bodies; b += gridDim.x * blockDim.x) {
+    const std::uint32_t begin = offsets[b];
+    const std::uint32_t k = offsets[b + 1] - begin;
+    if (k <= 1) continue;
+    if (k <= kRegisterEntries) {
+      std::uint32_t v[kRegisterEntries];
+#pragma unroll
+      for (std::uint32_t j = 0; j < kRegisterEntries; ++j) v[j] = j < k ? values[begin + j] : 0xFFFFFFFFu;
+      bitonic_sort_u32(v);
+#pragma unroll
+      for (std::uint32_t j = 0; j < kRegisterEntries; ++j) {
+        if (j < k) values[begin + j] = v[j];
+      }
+    } else if (k <= kLocalEntries) {
+      sort_local(values, begin, k);
+    } else {
+      sort_global(values, begin, k);
+    }
+  }
+}
+
+// The jacobian, lever and row of every entry (`total` entries: the last
+// body's end offset).
+__global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __restrict__ values,
+                                        const std::uint32_t* __restrict__ total, std::uint32_t rows,
                                         float4* __restrict__ out_a, float4* __restrict__ out_b,
                                         std::uint32_t* status) {
+  const std::uint32_t entries = *total;
   for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < entries; k += gridDim.x * blockDim.x) {
     const std::uint32_t v = values[k];
     const std::uint32_t row = v >> 1;
-    if (!index_ok(row, entries / 2, status)) continue;
+    if (!index_ok(row, rows, status)) continue;
     if (v & 1u) {
       const float4 c = r.c[row];
       const float4 d = r.d[row];
@@ -505,22 +589,24 @@ int bits_for(std::uint32_t value) {
 namespace {
 
 void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
-                    std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
-                    cudaStream_t stream, std::uint32_t* status) {
+                    std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp, cudaStream_t stream,
+                    std::uint32_t* status) {
+  // Counts per body, their scan, the entries scattered into their bodies'
+  // ranges, each range sorted by row, then the jacobians gathered.
   cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
   if (row_count > 0) {
-    incidence_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, body_count, keys,
-                                                                          values, counts);
+    incidence_counts_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, counts);
     count_launch();
   }
   exclusive_scan(counts, incidence.offsets, body_count + 1, temp, stream);
   if (row_count == 0) return;
-  const std::uint64_t n = 2ull * row_count;
-  radix_sort_pairs(keys, values, n, bits_for(body_count), temp, stream);
-  // A constraint row has no second entry; its key sorts past every body and
-  // the offsets end before it, so gathering all 2R entries is harmless.
-  incidence_gather_kernel<<<grid_for(n, 256), 256, 0, stream>>>(rows, values, std::uint32_t(n), incidence.a,
-                                                                 incidence.b, status);
+  incidence_scatter_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, incidence.offsets,
+                                                                          counts, values);
+  count_launch();
+  incidence_order_kernel<<<grid_for(body_count, 256), 256, 0, stream>>>(incidence.offsets, body_count, values);
+  count_launch();
+  incidence_gather_kernel<<<grid_for(2ull * row_count, 256), 256, 0, stream>>>(
+      rows, values, incidence.offsets + body_count, row_count, incidence.a, incidence.b, status);
   count_launch();
 }
 
@@ -529,7 +615,8 @@ void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_
 void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body_count, IncidenceArrays incidence,
                      std::uint32_t* keys, std::uint32_t* values, std::uint32_t* counts, std::uint32_t* temp,
                      cudaStream_t stream, std::uint32_t* status) {
-  incidence_pass(rows, row_count, body_count, incidence, keys, values, counts, temp, stream, status);
+  (void)keys;
+  incidence_pass(rows, row_count, body_count, incidence, values, counts, temp, stream, status);
 }
 
 void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,
