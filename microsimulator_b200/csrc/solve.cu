@@ -568,20 +568,21 @@ __global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __rest
   }
 }
 
-__global__ void keyed_keys_kernel(const uint2* __restrict__ slots, std::uint32_t rows, std::uint32_t* __restrict__ keys,
-                                  std::uint32_t* __restrict__ values, std::uint32_t* __restrict__ counts) {
+__global__ void keyed_counts_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
+                                    std::uint32_t* __restrict__ counts) {
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const std::uint32_t s = slots[i].x;
-    keys[i] = s;
-    values[i] = i;
-    atomicAdd(&counts[s], 1u);
+    atomicAdd(&counts[slots[i].x], 1u);
   }
 }
 
-int bits_for(std::uint32_t value) {
-  int bits = 0;
-  while (bits < 32 && (std::uint64_t(1) << bits) <= value) ++bits;
-  return bits;
+// Each row to a free place in its first slot's list (the counts run back to zero).
+__global__ void keyed_scatter_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
+                                     const std::uint32_t* __restrict__ offsets, std::uint32_t* __restrict__ counts,
+                                     std::uint32_t* __restrict__ rows_out) {
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
+    const std::uint32_t s = slots[i].x;
+    rows_out[offsets[s] + atomicSub(&counts[s], 1u) - 1u] = i;
+  }
 }
 
 }  // namespace
@@ -622,13 +623,20 @@ void build_incidence(RowArrays rows, std::uint32_t row_count, std::uint32_t body
 void build_keyed(const uint2* slots, std::uint32_t row_count, std::uint32_t body_count, std::uint32_t* offsets,
                  std::uint32_t* rows_out, std::uint32_t* keys, std::uint32_t* counts, std::uint32_t* temp,
                  cudaStream_t stream) {
+  // Counts per first slot, their scan, the rows scattered into their lists,
+  // each list sorted by row (a stable grouping, as KeyedRows keeps).
+  (void)keys;
   cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
   if (row_count > 0) {
-    keyed_keys_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(slots, row_count, keys, rows_out, counts);
+    keyed_counts_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(slots, row_count, counts);
     count_launch();
   }
   exclusive_scan(counts, offsets, body_count + 1, temp, stream);
-  if (row_count > 1) radix_sort_pairs(keys, rows_out, row_count, bits_for(body_count - 1), temp, stream);
+  if (row_count == 0) return;
+  keyed_scatter_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(slots, row_count, offsets, counts, rows_out);
+  count_launch();
+  incidence_order_kernel<<<grid_for(body_count, 256), 256, 0, stream>>>(offsets, body_count, rows_out);
+  count_launch();
 }
 
 SolveGraph::~SolveGraph() {
