@@ -41,7 +41,7 @@ __device__ void colony_body_pass(const BatchDesc& d, std::uint32_t b0, std::uint
 #pragma unroll
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
-          const std::uint32_t row = __float_as_uint(eb[t].w);
+          const std::uint32_t row = __float_as_uint(eb[t].w) >> 1;  // side bits: row << 1 | side
           gv[t] = __ldcg(&g[row]);
           pv[t] = project ? __ldcg(&gap[row]) : 0.0f;
         }

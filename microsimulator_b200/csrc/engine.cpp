@@ -507,6 +507,7 @@ struct msb_context {
   msb::DBuf<float4> body_a, body_b, drift_a, drift_b;
   msb::DBuf<std::uint32_t> inc_offsets;
   msb::DBuf<float4> inc_a, inc_b, resp_a, resp_b, accepted_a, accepted_b;
+  msb::DBuf<float2> inc_constants, inc_sides;  // per row: (offset, compliance), the two side terms
   msb::DBuf<float> slack;
 
   // A batch of independent colonies (msb_advance_contact_dynamics_batch);
@@ -979,12 +980,16 @@ bool use_fused_relaxation(Ctx& c, std::uint32_t items) {
   return items <= kFusedRelaxationItems;
 }
 
+IncidenceArrays incidence_arrays(Ctx& c) {
+  return {c.inc_offsets.p, c.inc_a.p, c.inc_b.p, c.inc_constants.p, c.inc_sides.p};
+}
+
 void fill_desc(Ctx& c, std::uint32_t row_count, float dt, const msb_growth_load_response& growth, float tolerance,
                std::uint32_t max_iterations, bool with_state = false) {
   SolveDesc& d = *c.host_desc;
   d.rows = c.rows.arrays();
   d.bodies = {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
-  d.incidence = {c.inc_offsets.p, c.inc_a.p, c.inc_b.p};
+  d.incidence = incidence_arrays(c);
   d.response = {c.resp_a.p, c.resp_b.p};
   d.multipliers = c.rows.multipliers.p;
   d.gaps = c.rows.gaps.p;
@@ -1028,11 +1033,13 @@ void build_system_incidence(Ctx& c, std::uint32_t row_count) {
   c.inc_offsets.ensure(c.n + 1ull);
   c.inc_a.ensure(entries);
   c.inc_b.ensure(entries);
+  c.inc_constants.ensure(entries / 2);
+  c.inc_sides.ensure(entries / 2);
   c.sort_keys.ensure(entries);
   c.sort_values.ensure(entries);
   c.counts.ensure(c.n + 1ull);
   c.temp.ensure(sort_temp_words(entries) + scan_temp_words(c.n + 1ull) + 64);
-  build_incidence(c.rows.arrays(), row_count, c.n, {c.inc_offsets.p, c.inc_a.p, c.inc_b.p}, c.sort_keys.p,
+  build_incidence(c.rows.arrays(), row_count, c.n, incidence_arrays(c), c.sort_keys.p,
                   c.sort_values.p, c.counts.p, c.temp.p, c.stream, c.scalars.p + kStatus);
 }
 
@@ -1076,6 +1083,9 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
     fill_desc(c, rows, dt, growth, tolerance, max_iterations);
     check(cudaError_t(graph.launch(c.stream)), "solve launch");
   }
+  // The response of the final multipliers (the passes of a solve write only
+  // the rows' side terms).
+  launch_evaluate(c.desc, c.last_blocks, false, c.stream);
   check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read desc");
   sync(c);
   const SolveDesc& d = *c.host_desc;
@@ -1095,7 +1105,7 @@ msb::BatchDesc batch_desc(Ctx& c, float dt, const msb_growth_load_response& grow
   msb::BatchDesc d{};
   d.rows = c.rows.arrays();
   d.bodies = {c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
-  d.incidence = {c.inc_offsets.p, c.inc_a.p, c.inc_b.p};
+  d.incidence = incidence_arrays(c);
   d.response = {c.resp_a.p, c.resp_b.p};
   d.multipliers = c.rows.multipliers.p;
   d.gaps = c.rows.gaps.p;
@@ -1358,7 +1368,7 @@ void guess_forces(Ctx& c, float dt, const msb_growth_load_response& growth) {
   const BodyArrays bodies{c.body_a.p, c.body_b.p, c.drift_a.p, c.drift_b.p};
   const ResponseArrays guess{c.guess_a.p, c.guess_b.p};
   launch_guess_response(n, c.guess.p, bodies, c.guess_dt, guess, c.stream);
-  launch_guess_forces(n, rows, {c.inc_offsets.p, c.inc_a.p, c.inc_b.p}, bodies, {c.resp_a.p, c.resp_b.p}, guess,
+  launch_guess_forces(n, rows, incidence_arrays(c), bodies, {c.resp_a.p, c.resp_b.p}, guess,
                       c.rows.slots.p, c.guess_delta.p, c.rows.multipliers.p, c.stream);
 }
 

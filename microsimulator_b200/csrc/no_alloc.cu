@@ -113,7 +113,7 @@ __device__ void small_body_pass(const SmallSolve& s, bool project, float alpha) 
     for (std::uint32_t k = s.incidence.offsets[b]; k < s.incidence.offsets[b + 1]; ++k) {
       const float4 ea = s.incidence.a[k];
       const float4 eb = s.incidence.b[k];
-      const std::uint32_t row = __float_as_uint(eb.w);
+      const std::uint32_t row = __float_as_uint(eb.w) >> 1;  // side bits: row << 1 | side
       const float g = s.multipliers[row];
       const float m = project ? smax(0.0f, g - alpha * s.gaps[row]) : g;
       if (m == 0.0f) continue;
@@ -395,7 +395,7 @@ extern "C" int msb_solve_contact_forces_no_alloc(const msb_contact_system* syste
   s.multipliers = carve.take<float>(rows);
   s.gaps = carve.take<float>(rows);
   s.incidence = {carve.take<std::uint32_t>(bodies + 1ull), carve.take<float4>(2ull * rows),
-                 carve.take<float4>(2ull * rows)};
+                 carve.take<float4>(2ull * rows), nullptr, nullptr};  // its own passes need no side terms
   std::uint32_t* keys = carve.take<std::uint32_t>(2ull * rows);
   std::uint32_t* values = carve.take<std::uint32_t>(2ull * rows);
   std::uint32_t* counts = carve.take<std::uint32_t>(bodies + 1ull);

@@ -6,9 +6,11 @@
 //   body pass  one thread per body sums its rows' projected multipliers
 //              times their jacobians in row order (the reference's
 //              incidence order, so a body's force and torque carry the same
-//              bits), then applies the mobility and the growth-load law;
-//   row pass   one thread per row forms the new gap, the FP64 BB products
-//              and the complementarity residual; the last block to finish
+//              bits), applies the mobility and the growth-load law, and
+//              stores each of its rows' side terms of the gap rate;
+//   row pass   one thread per row adds its two side terms into the new gap
+//              and forms the FP64 BB products and the complementarity
+//              residual; the last block to finish
 //              combines the per-block partials in block order (so the result
 //              does not depend on scheduling), sets the next step length and
 //              the convergence flag, and writes the flag into the WHILE node
@@ -66,7 +68,13 @@ constexpr int kBatch = MSB_BODY_BATCH;
 // so a body's force, torque and load carry the reference's bits.  The entries
 // are read kBatch at a time and their multiplier gathers issued together, so
 // that each thread keeps several independent loads in flight.
-// mode 0 and 2 evaluate the multipliers as they are; mode 1 their projection.
+// The thread then forms, for each of its entries, that side's term of the
+// row's gap rate (jacobian . velocity - lever * elongation rate, as row_gap
+// forms it, cpp/cpu/cpu_contact_dynamics.cpp:149-159) and stores it in the
+// row's side slot.  The row pass then adds a row's two terms instead of
+// reading its jacobians again and gathering both bodies' responses.
+// mode 0 and 2 evaluate the multipliers as they are, mode 1 their
+// projection; mode 2 (an evaluation, not a solve) also writes the response.
 // `Tag` only names a second instance of the same code for the timing hook,
 // so that a profiler can select its launches apart from the solve graph's.
 // Loads of data that other blocks write during a fused solve go through L2
@@ -80,7 +88,7 @@ __device__ __forceinline__ float shared_load(const float* p) {
   }
 }
 template <bool Coherent>
-__device__ __forceinline__ float4 shared_load(const float4* p) {
+__device__ __forceinline__ float2 shared_load(const float2* p) {
   if constexpr (Coherent) {
     return __ldcg(p);
   } else {
@@ -95,6 +103,9 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
   const float* __restrict__ g = d.multipliers;
   const float* __restrict__ gap = d.gaps;
   const std::uint32_t* __restrict__ offsets = d.incidence.offsets;
+  const float4* __restrict__ entry_a = d.incidence.a;
+  const float4* __restrict__ entry_b = d.incidence.b;
+  float* __restrict__ sides = reinterpret_cast<float*>(d.incidence.sides);
   for (std::uint32_t b = block * blockDim.x + threadIdx.x; b < d.body_count; b += blocks * blockDim.x) {
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float load = 0.0f;
@@ -103,20 +114,23 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
     if (!index_ok(end, std::uint64_t(2) * d.row_count + 1, check) || !index_ok(begin, std::uint64_t(end) + 1, check)) {
       end = begin;  // offsets out of range or not monotone: no entries
     }
+    // The batch of entries read last stays in registers for the side terms.
+    float4 ea[kBatch], eb[kBatch];
+    std::uint32_t last = begin;
     for (std::uint32_t k0 = begin; k0 < end; k0 += kBatch) {
-      float4 ea[kBatch], eb[kBatch];
+      last = k0;
       float gv[kBatch], pv[kBatch];
 #pragma unroll
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
-          ea[t] = __ldcs(&d.incidence.a[k0 + t]);
-          eb[t] = __ldcs(&d.incidence.b[k0 + t]);
+          ea[t] = entry_a[k0 + t];
+          eb[t] = entry_b[k0 + t];
         }
       }
 #pragma unroll
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
-          const std::uint32_t row = __float_as_uint(eb[t].w);
+          const std::uint32_t row = __float_as_uint(eb[t].w) >> 1;
           const bool ok = index_ok(row, d.row_count, check);
           gv[t] = ok ? shared_load<Coherent>(&g[row]) : 0.0f;
           pv[t] = ok && mode == 1 ? shared_load<Coherent>(&gap[row]) : 0.0f;
@@ -140,8 +154,30 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
     float v[6];
     float rate;
     respond(d, b, w, load, v, rate);
-    d.response.a[b] = make_float4(v[0], v[1], v[2], rate);
-    d.response.b[b] = make_float4(v[3], v[4], v[5], load);
+    if (mode == 2) {
+      // An evaluation: the response is the result.  Inside a solve only
+      // the side terms are needed; the solve ends with an evaluation of
+      // its final multipliers.
+      d.response.a[b] = make_float4(v[0], v[1], v[2], rate);
+      d.response.b[b] = make_float4(v[3], v[4], v[5], load);
+    }
+    // Each entry's side term of its row's rate: the entries before the last
+    // batch read again (a body with more than kBatch entries), then the
+    // last batch from registers.
+    const std::uint64_t side_count = std::uint64_t(2) * d.row_count;
+    for (std::uint32_t k = begin; k < last; ++k) {
+      const float4 a0 = __ldcs(&entry_a[k]);
+      const float4 b0 = __ldcs(&entry_b[k]);
+      const std::uint32_t s0 = __float_as_uint(b0.w);
+      if (index_ok(s0, side_count, check)) sides[s0] = side_term(a0, b0, v, rate);
+    }
+#pragma unroll
+    for (int t = 0; t < kBatch; ++t) {
+      if (last + t < end) {
+        const std::uint32_t side = __float_as_uint(eb[t].w);
+        if (index_ok(side, side_count, check)) sides[side] = side_term(ea[t], eb[t], v, rate);
+      }
+    }
   }
 }
 
@@ -162,33 +198,25 @@ __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode,
   const float dt = d.dt;
   float* __restrict__ g = d.multipliers;
   float* __restrict__ gap = d.gaps;
+  const float2* __restrict__ sides = d.incidence.sides;
+  const float2* __restrict__ constants = d.incidence.constants;
   double ss = 0.0, sy = 0.0, yy = 0.0;
   float residual = 0.0f;
   bool finite = true;
-  // row_gap (cpp/cpu/cpu_contact_dynamics.cpp:149-159): each side's
-  // jacobian . velocity - lever * elongation rate, summed in that order.
+  (void)check;
+  // row_gap (cpp/cpu/cpu_contact_dynamics.cpp:149-159): offset + dt * (first
+  // side's term + second side's term) + compliance * multiplier.  The body
+  // pass formed each side's term; a constraint row's second is -0.0f, and
+  // x + -0.0f == x, so the sum is the reference's bit for bit.
   const bool project = mode == 1;
   for (std::uint32_t i = block * blockDim.x + threadIdx.x; i < d.row_count; i += blocks * blockDim.x) {
     const float gi = shared_load<Coherent>(&g[i]);
     const float gpi = project ? shared_load<Coherent>(&gap[i]) : 0.0f;
-    const uint2 s = __ldcs(&d.rows.slots[i]);
-    if (!index_ok(s.x, d.body_count, check) || (s.y != kInvalidSlot && !index_ok(s.y, d.body_count, check))) continue;
-    const float4 ra = __ldcs(&d.rows.a[i]);
-    const float4 rb = __ldcs(&d.rows.b[i]);
-    const float4 rd = __ldcs(&d.rows.d[i]);
-    const float4 va = shared_load<Coherent>(&d.response.a[s.x]);
-    const float4 vb = shared_load<Coherent>(&d.response.b[s.x]);
+    const float2 side = shared_load<Coherent>(&sides[i]);
+    const float2 k = __ldcs(&constants[i]);
     const float m = project ? smax(0.0f, gi - alpha * gpi) : gi;
-    const float v1[6] = {va.x, va.y, va.z, vb.x, vb.y, vb.z};
-    float rate = side_term(ra, rb, v1, va.w);
-    if (s.y != kInvalidSlot) {
-      const float4 rc = __ldcs(&d.rows.c[i]);
-      const float4 wa = shared_load<Coherent>(&d.response.a[s.y]);
-      const float4 wb = shared_load<Coherent>(&d.response.b[s.y]);
-      const float v2[6] = {wa.x, wa.y, wa.z, wb.x, wb.y, wb.z};
-      rate += side_term(rc, rd, v2, wa.w);
-    }
-    const float gn = rb.w + dt * rate + rd.w * m;
+    const float rate = side.x + side.y;
+    const float gn = k.x + dt * rate + k.y * m;
     residual = smax(residual, row_residual(m, gn));
     finite = finite && isfinite(gn);
     if (project) {
@@ -446,13 +474,18 @@ __global__ void solve_reset_kernel(SolveDesc* desc) {
 // ------------------------------------------------------------- incidence
 
 // Entries per body: one for a row's first slot, one for its second (a
-// constraint row has none).
-__global__ void incidence_counts_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
-                                        std::uint32_t* __restrict__ counts) {
+// constraint row has none).  With `constants`, also each row's (offset,
+// compliance) and -0.0f as a constraint row's second side term.
+__global__ void incidence_counts_kernel(RowArrays r, std::uint32_t rows, std::uint32_t* __restrict__ counts,
+                                        float2* __restrict__ constants, float2* __restrict__ sides) {
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const uint2 s = slots[i];
+    const uint2 s = r.slots[i];
     atomicAdd(&counts[s.x], 1u);
     if (s.y != kInvalidSlot) atomicAdd(&counts[s.y], 1u);
+    if (constants != nullptr) {
+      constants[i] = make_float2(r.b[i].w, r.d[i].w);
+      if (s.y == kInvalidSlot) reinterpret_cast<float*>(sides)[2 * std::uint64_t(i) + 1] = -0.0f;
+    }
   }
 }
 
@@ -543,8 +576,8 @@ __global__ void incidence_order_kernel(const std::uint32_t* __restrict__ offsets
   }
 }
 
-// The jacobian, lever and row of every entry (`total` entries: the last
-// body's end offset).
+// The jacobian, lever and side bits (row << 1 | side) of every entry
+// (`total` entries: the last body's end offset).
 __global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __restrict__ values,
                                         const std::uint32_t* __restrict__ total, std::uint32_t rows,
                                         float4* __restrict__ out_a, float4* __restrict__ out_b,
@@ -558,12 +591,12 @@ __global__ void incidence_gather_kernel(RowArrays r, const std::uint32_t* __rest
       const float4 c = r.c[row];
       const float4 d = r.d[row];
       out_a[k] = c;
-      out_b[k] = make_float4(d.x, d.y, d.z, __uint_as_float(row));
+      out_b[k] = make_float4(d.x, d.y, d.z, __uint_as_float(v));
     } else {
       const float4 a = r.a[row];
       const float4 b = r.b[row];
       out_a[k] = a;
-      out_b[k] = make_float4(b.x, b.y, b.z, __uint_as_float(row));
+      out_b[k] = make_float4(b.x, b.y, b.z, __uint_as_float(v));
     }
   }
 }
@@ -596,7 +629,8 @@ void incidence_pass(RowArrays rows, std::uint32_t row_count, std::uint32_t body_
   // ranges, each range sorted by row, then the jacobians gathered.
   cudaMemsetAsync(counts, 0, (body_count + 1) * sizeof(std::uint32_t), stream);
   if (row_count > 0) {
-    incidence_counts_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows.slots, row_count, counts);
+    incidence_counts_kernel<<<grid_for(row_count, 256), 256, 0, stream>>>(rows, row_count, counts,
+                                                                         incidence.constants, incidence.sides);
     count_launch();
   }
   exclusive_scan(counts, incidence.offsets, body_count + 1, temp, stream);

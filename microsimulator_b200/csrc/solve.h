@@ -40,11 +40,20 @@ struct ResponseArrays {
 };
 
 // Per body, its rows in row order (CSR): entry a = jacobian 0..3,
-// entry b = jacobian 4, 5, lever, row index (bits).
+// entry b = jacobian 4, 5, lever, side (bits: row << 1 | 0 for the row's
+// first slot, 1 for its second).
+// Per row, for the BB passes (null where no BB pass runs on them):
+//   constants = (offset, compliance), written with the incidence;
+//   sides     = each side's term of the gap rate, jacobian . velocity -
+//               lever * elongation rate, indexed by the entries' side bits
+//               and written by the body pass.  A constraint row's second
+//               side holds -0.0f, which adds nothing: x + -0.0f == x.
 struct IncidenceArrays {
   std::uint32_t* offsets;
   float4* a;
   float4* b;
+  float2* constants;
+  float2* sides;
 };
 
 // Everything one solve reads and writes, in device memory at a fixed address
@@ -136,7 +145,9 @@ int relax_resident_blocks();
 constexpr unsigned long long kBarrierTimeoutNs = 5'000'000'000ull;
 
 // Evaluates the response of desc->multipliers once (no solve), as
-// evaluate_contact_response does; also the gaps when `with_gaps`.
+// evaluate_contact_response does; also the gaps when `with_gaps`.  A solve
+// writes no response itself: this evaluation of its final multipliers
+// follows it.
 void launch_evaluate(SolveDesc* desc, int blocks, bool with_gaps, cudaStream_t stream);
 
 // One more projected iteration of the last solved system (body pass then

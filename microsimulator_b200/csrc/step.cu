@@ -297,7 +297,7 @@ __global__ void guess_forces_body_kernel(std::uint32_t n, IncidenceArrays inc, B
     for (std::uint32_t k = begin; k < end; ++k) {
       const float4 ea = inc.a[k], eb = inc.b[k];
       const float u = ea.x * w[0] + ea.y * w[1] + ea.z * w[2] + ea.w * w[3] + eb.x * w[4] + eb.y * w[5];
-      const std::uint32_t row = __float_as_uint(eb.w);
+      const std::uint32_t row = __float_as_uint(eb.w) >> 1;  // side bits: row << 1 | side
       const float share = slots[row].y == kInvalidSlot ? 1.0f : 0.5f;
       // At most two additions onto zero per row: the sum does not depend on their order.
       atomicAdd(&delta[row], share * alpha * u);
