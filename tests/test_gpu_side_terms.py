@@ -1,0 +1,110 @@
+"""The BB passes split a row's gap into two side terms: the body pass stores
+jacobian . velocity - lever * elongation rate for each of its rows, and the
+row pass forms offset + dt * (first + second) + compliance * multiplier, with
+-0.0f as a constraint row's second term.  These systems mix pair and
+constraint rows, signed-zero offsets and multipliers, zero jacobians and
+levers, fixed bodies, drift and every growth law, and check gaps and
+responses bit for bit (as raw float bits, so the sign of a zero counts)
+against the reference library and the oracle (row_gap,
+cpp/cpu/cpu_contact_dynamics.cpp:149-159)."""
+
+import numpy as np
+import pytest
+
+from microsimulator_b200 import abi
+from microsimulator_b200.types import ContactSolveParameters, ContactSystem, GrowthLoadResponse
+
+pytestmark = pytest.mark.gpu
+
+LAWS = [
+    GrowthLoadResponse(0, 0.0, 0.0, 1.0),
+    GrowthLoadResponse(1, 0.4, 0.0, 1.0),
+    GrowthLoadResponse(2, 0.0, 0.2, 3.0),
+]
+
+
+def mixed_system(seed: int, bodies: int, rows: int, law: GrowthLoadResponse, walls: float = 0.3) -> ContactSystem:
+    rng = np.random.default_rng(seed)
+    r = np.zeros(rows, dtype=abi.CONTACT_ROW_DTYPE)
+    first = rng.integers(0, bodies, rows)
+    second = (first + rng.integers(1, bodies, rows)) % bodies
+    wall = rng.random(rows) < walls
+    r["first_slot"] = first
+    r["second_slot"] = np.where(wall, abi.INVALID_SLOT, second)
+    r["first_jacobian"] = rng.normal(0.0, 1.0, (rows, 6)).astype(np.float32)
+    r["second_jacobian"] = np.where(wall[:, None], 0.0, rng.normal(0.0, 1.0, (rows, 6))).astype(np.float32)
+    r["first_length_lever"] = rng.uniform(0.0, 0.5, rows).astype(np.float32)
+    r["second_length_lever"] = np.where(wall, 0.0, rng.uniform(0.0, 0.5, rows)).astype(np.float32)
+    r["offset"] = rng.normal(0.0, 0.05, rows).astype(np.float32)
+    r["compliance"] = rng.uniform(0.0, 0.2, rows).astype(np.float32)
+    # Edge values: signed-zero offsets, rows with zero compliance, a zero
+    # first jacobian and lever (the first side term is then +0.0f).
+    r["offset"][::7] = np.float32(-0.0)
+    r["offset"][3::7] = np.float32(0.0)
+    r["compliance"][::5] = 0.0
+    r["first_jacobian"][::11] = 0.0
+    r["first_length_lever"][::11] = 0.0
+    b = np.zeros(bodies, dtype=abi.CONTACT_BODY_DTYPE)
+    axis = rng.normal(0.0, 1.0, (bodies, 3))
+    b["axis"] = (axis / np.linalg.norm(axis, axis=1, keepdims=True)).astype(np.float32)
+    b["translational_mobility"] = rng.uniform(0.2, 1.0, bodies).astype(np.float32)
+    b["transverse_mobility"] = rng.uniform(0.1, 2.0, bodies).astype(np.float32)
+    b["axial_mobility"] = rng.uniform(0.1, 2.0, bodies).astype(np.float32)
+    b["length_rate"] = rng.choice(np.array([0.0, 0.5, 1.5, -0.25], np.float32), bodies)
+    fixed = rng.random(bodies) < 0.05
+    for name in ("translational_mobility", "transverse_mobility", "axial_mobility"):
+        b[name][fixed] = 0.0
+    b["drift"] = np.where(rng.random((bodies, 1)) < 0.3, rng.normal(0.0, 0.1, (bodies, 6)), 0.0).astype(np.float32)
+    return ContactSystem(r, b, 0.02, law)
+
+
+def multipliers_for(system: ContactSystem, seed: int) -> np.ndarray:
+    rng = np.random.default_rng(seed)
+    m = rng.uniform(0.0, 2.0, len(system.rows)).astype(np.float32)
+    m[::3] = 0.0
+    m[1::9] = np.float32(-0.0)
+    return m
+
+
+def bits(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32).view(np.uint32)
+
+
+@pytest.mark.parametrize("law", range(len(LAWS)))
+@pytest.mark.parametrize("seed,bodies,rows", [(1, 40, 90), (2, 3000, 9000), (3, 20000, 70000)])
+def test_gaps_and_response_bit_exact(backend, reference, oracle, law, seed, bodies, rows):
+    system = mixed_system(seed, bodies, rows, LAWS[law])
+    m = multipliers_for(system, seed + 100)
+    gaps = backend.evaluate_contact_gaps(system, m)
+    assert np.array_equal(bits(gaps), bits(reference.evaluate_contact_gaps(system, m)))
+    assert np.array_equal(bits(gaps), bits(oracle.evaluate_contact_gaps(system, m)))
+    response = backend.evaluate_contact_response(system, m)
+    expected = reference.evaluate_contact_response(system, m)
+    assert np.array_equal(bits(response.velocities), bits(expected.velocities))
+    assert np.array_equal(bits(response.loads), bits(expected.loads))
+    assert np.array_equal(bits(response.length_rates), bits(expected.length_rates))
+
+
+def test_constraint_rows_only(backend, reference):
+    system = mixed_system(4, 500, 1500, LAWS[1], walls=1.0)
+    m = multipliers_for(system, 5)
+    assert np.array_equal(bits(backend.evaluate_contact_gaps(system, m)),
+                          bits(reference.evaluate_contact_gaps(system, m)))
+
+
+def test_solve_then_gaps_of_its_multipliers(backend, reference):
+    # The side terms a solve's passes leave behind do not disturb the calls
+    # after it: its multipliers give the reference's gaps and response bit
+    # for bit.  (The response a solve itself leaves for the move is checked
+    # by the stepping tests, whose positions match the reference's.)
+    system = mixed_system(6, 2000, 5000, LAWS[2])
+    system.rows["offset"] = -np.abs(system.rows["offset"])
+    solved = backend.solve_contact_forces(system, np.zeros(len(system.rows), np.float32),
+                                          ContactSolveParameters(1e-4, 5000))
+    assert solved.report.status in (abi.SOLVE_CONVERGED, abi.SOLVE_ITERATION_LIMIT)
+    m = solved.multipliers
+    assert np.array_equal(bits(backend.evaluate_contact_gaps(system, m)),
+                          bits(reference.evaluate_contact_gaps(system, m)))
+    response = backend.evaluate_contact_response(system, m)
+    expected = reference.evaluate_contact_response(system, m)
+    assert np.array_equal(bits(response.velocities), bits(expected.velocities))
