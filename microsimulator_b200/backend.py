@@ -6,11 +6,19 @@ Every call runs on the GPU; there is no CPU path.  Errors come back as the
 exceptions the reference raises: ``ValueError`` for std::invalid_argument,
 ``OverflowError`` for std::overflow_error, ``abi.NativeError`` (a
 RuntimeError) for std::runtime_error and CUDA failures.
+
+The native calls release the GIL (ctypes does), so, as the reference's
+bindings do (cpp/python/native_call.hpp:19-84), a backend is marked busy for
+the length of each call and a call from another thread meanwhile raises
+RuntimeError("native object is in use by another thread") instead of racing
+on the context.
 """
 
 from __future__ import annotations
 
 import ctypes
+import functools
+import threading
 from ctypes import c_float, c_uint32, c_uint64, c_void_p
 
 import numpy as np
@@ -36,12 +44,46 @@ def device_count() -> int:
     return int(abi.load_library().msb_device_count())
 
 
+IN_USE = "native object is in use by another thread"
+
+
+def _exclusive(method):
+    """One call at a time per backend: the calling thread holds the
+    backend's busy lock for the call (re-entered by its own nested calls);
+    another thread's call raises RuntimeError, as BusyObjects::enter does."""
+
+    @functools.wraps(method)
+    def call(self, *args, **kwargs):
+        busy = self.__dict__.get("_busy")
+        if busy is None:
+            return method(self, *args, **kwargs)
+        if not busy.acquire(blocking=False):
+            raise abi.NativeError(abi.ERR_RUNTIME, IN_USE)
+        try:
+            return method(self, *args, **kwargs)
+        finally:
+            busy.release()
+
+    return call
+
+
+def _calls_exclusive(cls):
+    """Wraps every public method of `cls` in _exclusive."""
+    for name, member in list(vars(cls).items()):
+        if name.startswith("_") or isinstance(member, (staticmethod, classmethod)) or not callable(member):
+            continue
+        setattr(cls, name, _exclusive(member))
+    return cls
+
+
+@_calls_exclusive
 class B200Backend:
     """make_cuda_backend(device_index): one context, one stream, its buffers."""
 
     def __init__(self, device_index: int = 0, library=None):
         """`library`: a path to load instead of libmsb200.so (the checked
         build, ``build.CHECKED_OUTPUT``)."""
+        self._busy = threading.RLock()
         self._lib = abi.load_library(library)
         handle = c_void_p()
         status = self._lib.msb_context_create(device_index, ctypes.byref(handle))
