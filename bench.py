@@ -176,8 +176,10 @@ def ncu_traffic():
     return json.loads(path.read_text())
 
 
-def run_reference_sample(args, seconds, steps_cap):
-    """The reference CPU backend on a bounded sample of the workload."""
+def run_reference_sample(args, seconds, steps_cap, warm=2):
+    """The reference CPU backend on a bounded sample of the workload: `warm`
+    untimed steps (the overlap of the random start resolves in them), then
+    timed steps until `seconds` or `steps_cap`."""
     from microsimulator_b200 import workloads
     from oracle.native import REFERENCE_PATH, Reference
 
@@ -188,7 +190,7 @@ def run_reference_sample(args, seconds, steps_cap):
     handle = ref.world_create(world)
     try:
         plan_world = world.copy()
-        for step in range(2):  # the overlap of the random start resolves here
+        for step in range(warm):
             plan = divide(plan_world, step, args.seed)
             ref.world_divide(handle, plan.parents, plan.rotations)
             ref.world_step(handle, DT, dynamics())
@@ -198,7 +200,7 @@ def run_reference_sample(args, seconds, steps_cap):
         elapsed = 0.0
         steps = 0
         while steps < steps_cap and (elapsed < seconds or steps == 0):
-            plan = divide(plan_world, steps + 2, args.seed)
+            plan = divide(plan_world, steps + warm, args.seed)
             ref.world_divide(handle, plan.parents, plan.rotations)
             t0 = time.perf_counter()
             ref.world_step(handle, DT, dynamics())
@@ -210,7 +212,7 @@ def run_reference_sample(args, seconds, steps_cap):
         return {"value": cells_steps / elapsed, "unit": "cell-steps/s", "cores": ref.thread_count(),
                 "kind": "reference",
                 "sample": f"{args.cpu_cells} capsules of the same distribution and area fraction, "
-                          f"{steps} timed steps after 2 untimed, {elapsed:.1f} s"}
+                          f"{steps} timed steps after {warm} untimed, {elapsed:.1f} s"}
     finally:
         ref.world_destroy(handle)
 
@@ -230,7 +232,7 @@ def reference_arm(args):
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    sample = run_reference_sample(args, seconds=1e9, steps_cap=max(1, args.steps))
+    sample = run_reference_sample(args, seconds=1e9, steps_cap=max(1, args.steps), warm=max(2, args.warmup))
     if sample is None:
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmsref.so was not built"}))
         return
