@@ -366,21 +366,22 @@ int msb_contact_system_diagonal_bound(msb_context* context, const msb_contact_sy
 
 /* No counterpart in the reference.  The contact solve of
  * msb_solve_contact_forces for callers that cannot allocate device memory:
- * code running while a CUDA stream is being captured into a graph (where
- * cudaMalloc is not allowed), under an allocator policy that forbids new
- * device allocations, from a host callback, or in a real-time loop that must
- * not wait on the driver's allocator.  It needs no context and calls no
- * cudaMalloc, cudaFree or allocating library routine: every buffer lives in
- * one static 8 MiB device array that each GPU loading this library holds
- * until the process exits.  Limits: at most 16,384 rows and 8,192 bodies;
- * a larger system returns MSB_ERR_CAPACITY.  Inputs and outputs are host
- * arrays, as in msb_solve_contact_forces; work runs on `stream` (a
- * cudaStream_t, NULL for the default stream) of the current device.  All
- * calls share the static array: calls that overlap on the GPU race, so
- * serialize them.  The first call on a device looks up the array's device
- * address; make it before any stream capture.  The result agrees with
- * msb_solve_contact_forces to the solve tolerance (the BB products are
- * reduced in a different fixed order). */
+ * code under an allocator policy that forbids new device allocations after
+ * start-up (a pool sized once, a memory budget fixed by a host framework), or
+ * a real-time loop that must not wait on the driver's allocator.  It needs no
+ * context and calls no cudaMalloc, cudaFree or allocating library routine:
+ * every buffer lives in one static 8 MiB device array that each GPU loading
+ * this library holds until the process exits.  Limits: at most 16,384 rows
+ * and 8,192 bodies; a larger system returns MSB_ERR_CAPACITY.  Inputs and
+ * outputs are host arrays, as in msb_solve_contact_forces; work runs on
+ * `stream` (a cudaStream_t, NULL for the default stream) of the current
+ * device, and the call synchronises that stream before it returns, so it
+ * does not serve code inside a stream capture or a host callback.  All calls
+ * share the static array: calls that overlap on the GPU race, so serialize
+ * them.  The first call on a device looks up the array's device address.
+ * On MSB_ERR_CUDA, *report is left as it was and `multipliers` may hold part
+ * of the result.  The result agrees with msb_solve_contact_forces to the
+ * solve tolerance (the BB products are reduced in a different fixed order). */
 int msb_solve_contact_forces_no_alloc(const msb_contact_system* system, const float* initial_multipliers,
                                       const msb_contact_solve_parameters* parameters, float* multipliers,
                                       msb_contact_solve_report* report, void* stream);

@@ -1,7 +1,10 @@
 // An allocation-free variant of the contact solve, for callers that cannot
-// allocate device memory: code running inside a CUDA stream capture, under
-// an allocator that forbids cudaMalloc, from a host callback, or in a
-// real-time loop that must not pause for the driver's allocator.
+// allocate device memory: code under an allocator policy that forbids new
+// device allocations once it has started (a pool sized at start-up, or a
+// memory budget fixed by a host framework), and real-time loops that must not
+// pause for the driver's allocator.  It is not for stream capture or host
+// callbacks: it copies from pageable host arrays and synchronises `stream`
+// before it returns, which neither context allows.
 //
 // Every buffer the solve needs lives in one file-scope device array of
 // kScratchBytes (8 MiB), so systems are limited to kMaxRows rows and
@@ -11,13 +14,14 @@
 // that must start at zero are cleared on every call, and calls that overlap
 // on the GPU (from two threads, or on two streams without ordering) race on
 // it.  The first call on a device looks up the array's device address with
-// that device current; make that first call before any stream capture.
+// that device current.
 //
 // The solve is the same Barzilai-Borwein projected gradient as the main
-// path: the incidence is built by the shared scan and radix sort on the
-// static scratch, and one thread block runs the whole iteration loop (body
-// pass, row pass, a fixed-tree block reduction of the BB products, the step
-// length update) without returning to the host.
+// path, with the same per-body and per-row arithmetic (solve_math.cuh): the
+// incidence is built by the main path's counting scatter and per-body sort
+// by row on the static scratch, and one thread block runs the whole
+// iteration loop (body pass, row pass, a fixed-tree block reduction of the
+// BB products, the step length update) without returning to the host.
 
 #include <cfloat>
 #include <cmath>
@@ -28,6 +32,7 @@
 #include "device.cuh"
 #include "kernels.h"
 #include "solve.h"
+#include "solve_math.cuh"
 #include "step.h"
 #include "../../include/msb200.h"
 
@@ -67,45 +72,11 @@ struct SmallSolve {
   float stall_load;
   float tolerance;
   std::uint32_t max_iterations;
+  bool has_drift;  // read by respond(): the drift arrays hold something
 };
 
-__device__ __forceinline__ float small_growth_factor(const SmallSolve& s, float load) {
-  if (s.law == MSB_GROWTH_LAW_EXPONENTIAL) return float(exp(double(-s.sensitivity * smax(0.0f, load))));
-  if (s.law == MSB_GROWTH_LAW_LINEAR) {
-    return sclamp(1.0f - (load - s.free_load) / (s.stall_load - s.free_load), 0.0f, 1.0f);
-  }
-  return 1.0f;
-}
-
-__device__ __forceinline__ float small_wrench_dot(float4 ja, float4 jb, float4 va, float4 vb) {
-  float r = 0.0f;
-  r += ja.x * va.x;
-  r += ja.y * va.y;
-  r += ja.z * va.z;
-  r += ja.w * vb.x;
-  r += jb.x * vb.y;
-  r += jb.y * vb.z;
-  return r;
-}
-
-// apply_mobility of one jacobian, dotted with itself (the diagonal entry).
-__device__ __forceinline__ float small_diagonal(float4 ja, float4 jb, float4 ba, float4 bb) {
-  const F3 axis{ba.x, ba.y, ba.z};
-  const F3 tq{ja.w, jb.x, jb.y};
-  const float s = (bb.y - bb.x) * dot(axis, tq);
-  const F3 ang = tq * bb.x + axis * s;
-  float r = 0.0f;
-  r += ja.x * (ja.x * ba.w);
-  r += ja.y * (ja.y * ba.w);
-  r += ja.z * (ja.z * ba.w);
-  r += ja.w * ang.x;
-  r += jb.x * ang.y;
-  r += jb.y * ang.z;
-  return r;
-}
-
 // Per body: the wrench of its rows' multipliers in row order, then the
-// mobility, drift and loaded elongation rate.
+// mobility, drift and loaded elongation rate (respond, as the main path).
 __device__ void small_body_pass(const SmallSolve& s, bool project, float alpha) {
   for (std::uint32_t b = threadIdx.x; b < s.body_count; b += blockDim.x) {
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
@@ -125,25 +96,28 @@ __device__ void small_body_pass(const SmallSolve& s, bool project, float alpha) 
       w[5] += m * eb.y;
       load += eb.z * m;
     }
-    const float4 ba = s.bodies.a[b];
-    const float4 bb = s.bodies.b[b];
-    const float4 da = s.bodies.drift_a[b];
-    const float4 db = s.bodies.drift_b[b];
-    const F3 axis{ba.x, ba.y, ba.z};
-    const F3 tq{w[3], w[4], w[5]};
-    const float sc = (bb.y - bb.x) * dot(axis, tq);
-    const F3 ang = tq * bb.x + axis * sc;
-    float v[6] = {w[0] * ba.w, w[1] * ba.w, w[2] * ba.w, ang.x, ang.y, ang.z};
-    v[0] += da.x;
-    v[1] += da.y;
-    v[2] += da.z;
-    v[3] += db.x;
-    v[4] += db.y;
-    v[5] += db.z;
-    const float rate = bb.z > 0.0f ? bb.z * small_growth_factor(s, load) : bb.z;
+    float v[6];
+    float rate;
+    respond(s, b, w, load, v, rate);
     s.response.a[b] = make_float4(v[0], v[1], v[2], rate);
     s.response.b[b] = make_float4(v[3], v[4], v[5], load);
   }
+}
+
+// One side's term of a row's gap rate from a body's stored response.
+__device__ __forceinline__ float small_side(float4 ja, float4 jb, float4 ra, float4 rb) {
+  const float v[6] = {ra.x, ra.y, ra.z, rb.x, rb.y, rb.z};
+  return side_term(ja, jb, v, ra.w);
+}
+
+// row_gap (cpu_contact_dynamics.cpp:149-159) of row i with multiplier m.
+__device__ __forceinline__ float small_gap(const SmallSolve& s, std::uint32_t i, float m) {
+  const uint2 sl = s.rows.slots[i];
+  const float4 rb = s.rows.b[i];
+  const float4 rd = s.rows.d[i];
+  float rate = small_side(s.rows.a[i], rb, s.response.a[sl.x], s.response.b[sl.x]);
+  if (sl.y != kInvalidSlot) rate += small_side(s.rows.c[i], rd, s.response.a[sl.y], s.response.b[sl.y]);
+  return rb.w + s.dt * rate + rd.w * m;
 }
 
 // Fixed-tree block reduction of five values (three sums, a max, a min).
@@ -181,9 +155,9 @@ __global__ void __launch_bounds__(kBlock) small_solve_kernel(SmallSolve s) {
   float bound = 0.0f;
   for (std::uint32_t i = threadIdx.x; i < s.row_count; i += blockDim.x) {
     const uint2 sl = s.rows.slots[i];
-    float entry = small_diagonal(s.rows.a[i], s.rows.b[i], s.bodies.a[sl.x], s.bodies.b[sl.x]);
+    float entry = diagonal(s.rows.a[i], s.rows.b[i], s.bodies.a[sl.x], s.bodies.b[sl.x]);
     const float4 rd = s.rows.d[i];
-    if (sl.y != kInvalidSlot) entry += small_diagonal(s.rows.c[i], rd, s.bodies.a[sl.y], s.bodies.b[sl.y]);
+    if (sl.y != kInvalidSlot) entry += diagonal(s.rows.c[i], rd, s.bodies.a[sl.y], s.bodies.b[sl.y]);
     bound = smax(bound, s.dt * entry + rd.w);
   }
   {
@@ -209,17 +183,9 @@ __global__ void __launch_bounds__(kBlock) small_solve_kernel(SmallSolve s) {
     bool finite = true;
     for (std::uint32_t i = threadIdx.x; i < s.row_count; i += blockDim.x) {
       const float m = s.multipliers[i];
-      const uint2 sl = s.rows.slots[i];
-      const float4 ra = s.rows.a[i];
-      const float4 rb = s.rows.b[i];
-      float rate = small_wrench_dot(ra, rb, s.response.a[sl.x], s.response.b[sl.x]) - rb.z * s.response.a[sl.x].w;
-      const float4 rd = s.rows.d[i];
-      if (sl.y != kInvalidSlot) {
-        rate += small_wrench_dot(s.rows.c[i], rd, s.response.a[sl.y], s.response.b[sl.y]) - rd.z * s.response.a[sl.y].w;
-      }
-      const float gap = rb.w + s.dt * rate + rd.w * m;
+      const float gap = small_gap(s, i, m);
       s.gaps[i] = gap;
-      residual = smax(residual, m > 0.0f ? fabsf(gap) : smax(0.0f, -gap));
+      residual = smax(residual, row_residual(m, gap));
       finite = finite && isfinite(gap);
     }
     double v[5] = {0.0, 0.0, 0.0, double(residual), finite ? 1.0 : 0.0};
@@ -252,21 +218,13 @@ __global__ void __launch_bounds__(kBlock) small_solve_kernel(SmallSolve s) {
       const float gi = s.multipliers[i];
       const float gpi = s.gaps[i];
       const float m = smax(0.0f, gi - alpha * gpi);
-      const uint2 sl = s.rows.slots[i];
-      const float4 ra = s.rows.a[i];
-      const float4 rb = s.rows.b[i];
-      float rate = small_wrench_dot(ra, rb, s.response.a[sl.x], s.response.b[sl.x]) - rb.z * s.response.a[sl.x].w;
-      const float4 rd = s.rows.d[i];
-      if (sl.y != kInvalidSlot) {
-        rate += small_wrench_dot(s.rows.c[i], rd, s.response.a[sl.y], s.response.b[sl.y]) - rd.z * s.response.a[sl.y].w;
-      }
-      const float gn = rb.w + s.dt * rate + rd.w * m;
+      const float gn = small_gap(s, i, m);
       const double moved = double(m) - double(gi);
       const double change = double(gn) - double(gpi);
       ss += moved * moved;
       sy += moved * change;
       yy += change * change;
-      residual = smax(residual, m > 0.0f ? fabsf(gn) : smax(0.0f, -gn));
+      residual = smax(residual, row_residual(m, gn));
       finite = finite && isfinite(gn);
       s.multipliers[i] = m;
       s.gaps[i] = gn;
@@ -284,12 +242,7 @@ __global__ void __launch_bounds__(kBlock) small_solve_kernel(SmallSolve s) {
         s.state->status = MSB_SOLVE_CONVERGED;
       } else {
         s.state->status = MSB_SOLVE_ITERATION_LIMIT;
-        float next = alpha_shared;
-        if (v[1] > 0.0 && v[2] > 0.0) {
-          const double candidate = (iteration % 2u) == 1u ? v[0] / v[1] : v[1] / v[2];
-          if (isfinite(candidate) && candidate > 0.0) next = float(candidate);
-        }
-        alpha_shared = next;
+        alpha_shared = next_step(alpha_shared, v[0], v[1], v[2], iteration);
         proceed = iteration < s.max_iterations ? 1 : 0;
       }
       proceed_shared = proceed;
@@ -364,8 +317,10 @@ extern "C" int msb_solve_contact_forces_no_alloc(const msb_contact_system* syste
     if (!valid_row(system->rows[r], bodies)) return MSB_ERR_INVALID_ARGUMENT;
     if (!std::isfinite(initial_multipliers[r]) || initial_multipliers[r] < 0.0f) return MSB_ERR_INVALID_ARGUMENT;
   }
-  *report = {MSB_SOLVE_CONVERGED, 0, 0.0f};
-  if (rows == 0) return MSB_OK;
+  if (rows == 0) {
+    *report = {MSB_SOLVE_CONVERGED, 0, 0.0f};
+    return MSB_OK;
+  }
 
   // Set-up, once per device with that device current: the device address
   // of the static scratch.
@@ -396,10 +351,11 @@ extern "C" int msb_solve_contact_forces_no_alloc(const msb_contact_system* syste
   s.gaps = carve.take<float>(rows);
   s.incidence = {carve.take<std::uint32_t>(bodies + 1ull), carve.take<float4>(2ull * rows),
                  carve.take<float4>(2ull * rows), nullptr, nullptr};  // its own passes need no side terms
-  std::uint32_t* keys = carve.take<std::uint32_t>(2ull * rows);
+  // The incidence build needs per-entry values, per-body counts and the
+  // scan's scratch; it takes no sort keys.
   std::uint32_t* values = carve.take<std::uint32_t>(2ull * rows);
   std::uint32_t* counts = carve.take<std::uint32_t>(bodies + 1ull);
-  std::uint32_t* temp = carve.take<std::uint32_t>(sort_temp_words(2ull * rows) + scan_temp_words(bodies + 1ull) + 64);
+  std::uint32_t* temp = carve.take<std::uint32_t>(scan_temp_words(bodies + 1ull) + 64);
   s.response = {carve.take<float4>(std::max<std::uint32_t>(bodies, 1)), carve.take<float4>(std::max<std::uint32_t>(bodies, 1))};
   s.state = carve.take<SmallState>(1);
   if (carve.used > kScratchBytes) return MSB_ERR_CAPACITY;
@@ -412,6 +368,10 @@ extern "C" int msb_solve_contact_forces_no_alloc(const msb_contact_system* syste
   s.stall_load = g.stall_load;
   s.tolerance = parameters->tolerance;
   s.max_iterations = parameters->max_iterations;
+  s.has_drift = false;
+  for (std::uint32_t b = 0; b < bodies && !s.has_drift; ++b) {
+    for (float v : system->bodies[b].drift) s.has_drift = s.has_drift || v != 0.0f || std::signbit(v);
+  }
 
   if (bodies > 0) {
     if (cudaMemcpyAsync(records, system->bodies, bodies * sizeof(msb_contact_body), cudaMemcpyHostToDevice, stream) !=
@@ -427,9 +387,11 @@ extern "C" int msb_solve_contact_forces_no_alloc(const msb_contact_system* syste
     return MSB_ERR_CUDA;
   }
   launch_rows_from_records(records, rows, s.rows, stream);
-  build_incidence(s.rows, rows, bodies, s.incidence, keys, values, counts, temp, stream);
+  build_incidence(s.rows, rows, bodies, s.incidence, nullptr, values, counts, temp, stream);
   small_solve_kernel<<<1, kBlock, 0, stream>>>(s);
   count_launch();
+  // On a CUDA error `multipliers` may already hold part of the device copy
+  // and *report is left as it was.
   SmallState state{};
   if (cudaGetLastError() != cudaSuccess ||
       cudaMemcpyAsync(&state, s.state, sizeof(state), cudaMemcpyDeviceToHost, stream) != cudaSuccess ||
