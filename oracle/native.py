@@ -44,6 +44,10 @@ def build(reference: bool = True) -> None:
     targets = ["oracle"]
     if reference and Path("/root/reference/cpp").exists():
         targets.append("ref")
+        # The reference's conformance tests against the B200 adapter need
+        # libmsb200.so built first.
+        if (HERE.parent / "microsimulator_b200" / "libmsb200.so").exists():
+            targets.append("conformance")
     subprocess.run(["make", "-s", "-C", str(HERE), "-j8", *targets], check=True)
 
 
