@@ -187,10 +187,11 @@ def test_colony_step_matches_reference(backend, golden, oracle):
     # Same substep structure as the reference.
     assert result.report.substeps == report[0]
     assert result.report.halvings == report[1]
-    # Positions within 1e-4 capsule radius of the reference are asserted at a
-    # tight tolerance below; at this tolerance the spread is reported.
+    # Both solves converge to the overlap tolerance (5e-4 um) from the same
+    # rows, so the positions agree to a few tolerances (measured on B200:
+    # 5.7e-4 um); 1e-4 capsule radius is asserted at a tight tolerance below.
     spread = np.max(np.abs(world.geometry()[:, :3] - stepped.geometry()[:, :3]))
-    assert spread < 0.05 * RADIUS, spread
+    assert spread <= 4 * 5e-4, spread
 
 
 @pytest.mark.parametrize("seed", [1, 2])
@@ -222,7 +223,8 @@ def test_step_with_trap_walls_matches_oracle(backend, oracle):
     ra = backend.advance_contact_dynamics(a, cs, 0.02, p)
     rb = oracle.advance_contact_dynamics(b, cs, 0.02, p)
     assert ra.report.substeps == rb.report.substeps
-    assert np.max(np.abs(a.geometry() - b.geometry())) < 0.05
+    # Within a few solve tolerances (measured on B200: identical bits).
+    assert np.max(np.abs(a.geometry() - b.geometry())) <= 4 * p.overlap_tolerance
 
 
 def test_device_resident_step_equals_host_step(backend):

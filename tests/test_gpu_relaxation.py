@@ -73,7 +73,8 @@ def test_fused_steps_with_walls(forms, oracle):
     ra = forms.advance_contact_dynamics(a, walls, 0.02, p)
     rb = oracle.advance_contact_dynamics(b, walls, 0.02, p)
     assert ra.report.substeps == rb.report.substeps
-    assert np.max(np.abs(a.geometry() - b.geometry())) < 0.05
+    # Within a few solve tolerances of the reference-identical oracle.
+    assert np.max(np.abs(a.geometry() - b.geometry())) <= 4 * p.overlap_tolerance
 
 
 def test_invalid_form(forms):
