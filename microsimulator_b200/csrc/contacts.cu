@@ -33,19 +33,13 @@ __global__ void cell_bounds_kernel(GeometryView g, float margin, double* __restr
   double high[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
   double width[3] = {0.0, 0.0, 0.0};
   double finite = 1.0;
-  const double margin_per_cell = double(margin) * 0.5;
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < g.count; i += gridDim.x * blockDim.x) {
-    const float4 pl = g.pos_len[i];
-    const float4 dr = g.dir_rad[i];
-    const double half = double(pl.w) * 0.5;
-    const double pad = double(dr.w) + margin_per_cell;
-    const double c[3] = {double(pl.x), double(pl.y), double(pl.z)};
-    const double d[3] = {double(dr.x), double(dr.y), double(dr.z)};
+    double box[6];
+    padded_box(g.pos_len[i], g.dir_rad[i], margin, box);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-      const double e = fabs(d[a]) * half + pad;
-      const double lo = c[a] - e;
-      const double hi = c[a] + e;
+      const double lo = box[a];
+      const double hi = box[3 + a];
       bounds[6 * std::uint64_t(i) + a] = lo;
       bounds[6 * std::uint64_t(i) + 3 + a] = hi;
       if (!isfinite(lo) || !isfinite(hi)) finite = 0.0;
@@ -214,10 +208,6 @@ __global__ void scatter_cells_kernel(GeometryView g, const double* __restrict__ 
     sorted_hi[at] = make_float4(__double2float_ru(box[3]), __double2float_ru(box[4]), __double2float_ru(box[5]), 0.0f);
     sorted_id[at] = g.ids[i];
   }
-}
-
-__device__ __forceinline__ bool boxes_overlap(const double* l, const double* r) {
-  return l[3] >= r[0] && r[3] >= l[0] && l[4] >= r[1] && r[4] >= l[1] && l[5] >= r[2] && r[5] >= l[2];
 }
 
 constexpr int kLocalPartners = 32;
@@ -520,6 +510,18 @@ __global__ void narrow_phase_kernel(GeometryView g, const uint2* __restrict__ pa
     if (!index_ok(pair.x, g.count, status) || !index_ok(pair.y, g.count, status)) {
       if (counts != nullptr) counts[k] = 0;
       continue;
+    }
+    if (prm.box_margin >= 0.0f) {
+      // Candidates from a wider search (or from another geometry): only
+      // the pairs whose boxes at box_margin overlap here are the
+      // reference's candidates.
+      double first[6], second[6];
+      padded_box(g.pos_len[pair.x], g.dir_rad[pair.x], prm.box_margin, first);
+      padded_box(g.pos_len[pair.y], g.dir_rad[pair.y], prm.box_margin, second);
+      if (!boxes_overlap(first, second)) {
+        if (counts != nullptr) counts[k] = 0;
+        continue;
+      }
     }
     const Capsule p = capsule_at(g, pair.x);
     const Capsule q = capsule_at(g, pair.y);

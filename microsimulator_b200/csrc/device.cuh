@@ -55,6 +55,29 @@ __device__ __forceinline__ bool normalized(F3 v, F3& out) {
 }
 __device__ __forceinline__ F3 xyz(float4 v) { return {v.x, v.y, v.z}; }
 
+// A capsule's FP64 box padded by half the margin on every side, as
+// find_cell_contact_candidates forms it (cpp/core/contact_graph.cpp:17-34):
+// centre -+ (|axis| * length / 2 + radius + margin / 2) per axis, into
+// box[0..2] (low) and box[3..5] (high).  Every box test of the contact search
+// goes through this one expression, so the boxes carry the same bits.
+__device__ __forceinline__ void padded_box(float4 pos_len, float4 dir_rad, float margin, double box[6]) {
+  const double half = double(pos_len.w) * 0.5;
+  const double pad = double(dir_rad.w) + double(margin) * 0.5;
+  const double c[3] = {double(pos_len.x), double(pos_len.y), double(pos_len.z)};
+  const double d[3] = {double(dir_rad.x), double(dir_rad.y), double(dir_rad.z)};
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const double e = fabs(d[a]) * half + pad;
+    box[a] = c[a] - e;
+    box[3 + a] = c[a] + e;
+  }
+}
+
+// The reference's box overlap test, touching included (contact_graph.cpp:37-41).
+__device__ __forceinline__ bool boxes_overlap(const double* l, const double* r) {
+  return l[3] >= r[0] && r[3] >= l[0] && l[4] >= r[1] && r[4] >= l[1] && l[5] >= r[2] && r[5] >= l[2];
+}
+
 __device__ __forceinline__ void raise_status(std::uint32_t* status, std::uint32_t code) {
   atomicCAS(status, 0u, code);
 }

@@ -162,6 +162,7 @@ enum Scalar : int {
   kRotationBits = 2,
   kInvalid = 3,
   kGrowthBits = 4,
+  kDisplacementBits = 5,
   kScalarCount = 16
 };
 
@@ -187,6 +188,10 @@ constexpr std::uint32_t kWarmFlags = kWarmCarry | kWarmGuess | kWarmLearned;
 // 24 against 28 us at 100k, 19 against 22 us at 20k), so automatic is the
 // graph.
 constexpr std::uint32_t kFusedRelaxationItems = 0;
+// The substep's first search pads its candidate boxes by this much more
+// than the candidate margin, so that its candidates serve the overlap
+// re-checks while no box face has moved more than half the padded margin.
+constexpr float kRecheckReach = 0.1f;
 constexpr float kMaximumSubstepRotation = 0.5f;
 constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
 
@@ -469,6 +474,15 @@ struct msb_context {
   msb::DBuf<std::uint32_t> cand_counts, cand_offsets, pair_counts, pair_offsets, wall_counts, wall_offsets;
   msb::DBuf<uint2> pairs;
   msb::DBuf<std::uint32_t> slab;  // the broad phase's kept partners, kSlabPartners per cell
+  // The candidate pairs of the current substep's first search (boxes padded
+  // by kept_margin at the substep's base geometry), which the overlap
+  // re-checks of its refinement rounds reuse while the cells have moved less
+  // than half of kept_margin (flag_overlaps).
+  msb::DBuf<uint2> kept_pairs;
+  std::uint32_t kept_count = 0;
+  float kept_margin = 0.0f;
+  bool kept_valid = false;
+  float displacement = 0.0f;  // the last move's largest box-face displacement
   msb::DBuf<msb::Touch> touches, found, flagged;
   msb::DBuf<std::uint32_t> flags, flag_offsets;
   msb::DBuf<msb::DeviceConstraint> constraints;
@@ -496,7 +510,7 @@ struct msb_context {
   bool has_guess = false;
   std::uint32_t guess_cells = 0;
   float guess_dt = 0.0f;
-  bool has_drift = false;  // a loaded system with some non-zero drift
+  bool has_drift = false;  // a loaded system with some drift other than +0.0f
   // The flow field of msb_set_flow_field, for steps with flow drift.
   bool has_flow = false;
   msb::FlowField flow{};
@@ -843,16 +857,46 @@ void load_constraints(Ctx& c, const msb_constraint* constraints, std::uint64_t c
 
 // ---- contact search ------------------------------------------------------
 
-// Cell-pair touches of `geometry` into c.touches[0, count); returns count.
-std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DBuf<Touch>& out) {
+// Touches at prm.margin among the candidate pairs in c.pairs[0, pair_count):
+// a count pass, its scan and a fill pass into out[0, count); returns count.
+std::uint32_t narrow_touches(Ctx& c, const GeometryView& g, ContactSearchParams prm, const uint2* pairs,
+                             std::uint32_t pair_count, DBuf<Touch>& out) {
+  if (pair_count == 0) return 0;
+  c.pair_counts.ensure(pair_count + 1ull);
+  c.pair_offsets.ensure(pair_count + 1ull);
+  c.temp.ensure(scan_temp_words(pair_count + 1ull) + 64);
+  check(cudaMemsetAsync(c.pair_counts.p + pair_count, 0, 4, c.stream), "memset");
+  launch_narrow_phase(g, pairs, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream, c.scalars.p + kStatus);
+  exclusive_scan(c.pair_counts.p, c.pair_offsets.p, pair_count + 1ull, c.temp.p, c.stream);
+  const std::uint32_t touch_count = read_u32(c, c.pair_offsets.p + pair_count);
+  read_scalars(c);
+  if (touch_count == 0) return 0;
+  out.ensure(touch_count + 1ull);
+  launch_narrow_phase(g, pairs, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream, c.scalars.p + kStatus);
+  return touch_count;
+}
+
+// Cell-pair touches of `geometry` at prm.margin into out[0, count); returns
+// count.  The broad phase pads the boxes by `candidate_margin` >= prm.margin;
+// with a wider one the narrow phase first applies the box test at
+// prm.margin, so the touches are those of a search at prm.margin.  With
+// `keep` the candidate pairs stay in c.kept_pairs.
+std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DBuf<Touch>& out,
+                         float candidate_margin = -1.0f, bool keep = false) {
+  candidate_margin = std::max(candidate_margin, prm.margin);
   const std::uint32_t n = c.n;
+  if (keep) {
+    c.kept_valid = true;
+    c.kept_count = 0;
+    c.kept_margin = candidate_margin;
+  }
   if (n < 2) return 0;
   const GeometryView g = view_of(c, geometry);
   const std::uint32_t partials = bound_partials(n);
   c.bounds.ensure(6ull * n);
   c.bound_partials.ensure(10ull * partials);
   c.grid.ensure(1);
-  launch_cell_bounds(g, prm.margin, c.bounds.p, c.bound_partials.p, c.stream);
+  launch_cell_bounds(g, candidate_margin, c.bounds.p, c.bound_partials.p, c.stream);
   const std::uint64_t capacity = grid_bucket_capacity(n);
   launch_grid_setup(c.bound_partials.p, partials, n, capacity, c.grid.p, c.stream, c.box_scale, c.colonies);
   c.cell_bucket.ensure(n);
@@ -901,19 +945,12 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
                        c.coords.p, c.rank.p, c.cand_counts.p, c.cand_offsets.p, c.pairs.p, c.scalars.p + kStatus,
                        c.stream, c.slab.p);
   }
-  c.pair_counts.ensure(pair_count + 1ull);
-  c.pair_offsets.ensure(pair_count + 1ull);
-  c.temp.ensure(scan_temp_words(pair_count + 1ull) + scan_temp_words(capacity) + sort_temp_words(n) + 64);
-  check(cudaMemsetAsync(c.pair_counts.p + pair_count, 0, 4, c.stream), "memset");
-  launch_narrow_phase(g, c.pairs.p, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream,
-                      c.scalars.p + kStatus);
-  exclusive_scan(c.pair_counts.p, c.pair_offsets.p, pair_count + 1ull, c.temp.p, c.stream);
-  const std::uint32_t touch_count = read_u32(c, c.pair_offsets.p + pair_count);
-  read_scalars(c);
-  if (touch_count == 0) return 0;
-  out.ensure(touch_count + 1ull);
-  launch_narrow_phase(g, c.pairs.p, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream,
-                      c.scalars.p + kStatus);
+  if (candidate_margin > prm.margin) prm.box_margin = prm.margin;
+  const std::uint32_t touch_count = narrow_touches(c, g, prm, c.pairs.p, pair_count, out);
+  if (keep) {
+    std::swap(c.pairs, c.kept_pairs);
+    c.kept_count = pair_count;
+  }
   return touch_count;
 }
 
@@ -939,12 +976,37 @@ std::uint32_t find_walls(Ctx& c, Geometry& geometry, float margin, float epsilon
 }
 
 // find_touches (contact_dynamics.cpp:176-210): pairs then constraint faces.
+// With `keep` the pair search's candidates (at `candidate_margin`, at least
+// `margin`) stay for the substep's re-checks.
 std::uint32_t find_touches(Ctx& c, Geometry& geometry, const msb_contact_parameters& cp,
-                           const msb_constraint_contact_parameters& wp, float margin, DBuf<Touch>& out) {
+                           const msb_constraint_contact_parameters& wp, float margin, DBuf<Touch>& out,
+                           float candidate_margin = -1.0f, bool keep = false) {
   const ContactSearchParams prm{margin, cp.parallel_sine_threshold, cp.degeneracy_epsilon};
-  const std::uint32_t pairs = find_pairs(c, geometry, prm, out);
+  const std::uint32_t pairs = find_pairs(c, geometry, prm, out, candidate_margin, keep);
   const std::uint32_t walls = find_walls(c, geometry, margin, wp.degeneracy_epsilon, true, out, pairs);
   return pairs + walls;
+}
+
+// The touches of find_touches at margin 0 on `geometry`, with the pair
+// candidates taken from the substep's kept list instead of a new search.
+// Exact when no cell's box face moved more than (kept_margin - 1e-6) / 2
+// since the kept search: a pair missing from the list had boxes padded by
+// kept_margin that did not overlap, so their unpadded boxes, each moved by
+// less than half of that, still do not, and the pair is no candidate of the
+// search at margin 0 either.  Listed pairs get that search's box test here.
+std::uint32_t find_touches_kept(Ctx& c, Geometry& geometry, const msb_contact_parameters& cp,
+                                const msb_constraint_contact_parameters& wp, DBuf<Touch>& out) {
+  ContactSearchParams prm{0.0f, cp.parallel_sine_threshold, cp.degeneracy_epsilon};
+  prm.box_margin = 0.0f;
+  const std::uint32_t pairs = narrow_touches(c, view_of(c, geometry), prm, c.kept_pairs.p, c.kept_count, out);
+  const std::uint32_t walls = find_walls(c, geometry, 0.0f, wp.degeneracy_epsilon, true, out, pairs);
+  return pairs + walls;
+}
+
+// Whether the last move allows find_touches_kept.
+bool kept_candidates_hold(const Ctx& c) {
+  return c.kept_valid && c.colonies == 0 && std::isfinite(c.displacement) &&
+         2.0 * double(c.displacement) <= double(c.kept_margin) - 1.0e-6;
 }
 
 // ---- solve ---------------------------------------------------------------
@@ -1243,7 +1305,8 @@ Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_const
                        const msb_contact_dynamics_parameters& p) {
   Overlaps o;
   mark(c, kPhaseSearch);
-  o.candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
+  o.candidates = kept_candidates_hold(c) ? find_touches_kept(c, c.state, cp, wp, c.found)
+                                         : find_touches(c, c.state, cp, wp, 0.0f, c.found);
   mark(c, kPhaseMove);
   c.flags.ensure(o.candidates + 1ull);
   c.flag_offsets.ensure(o.candidates + 1ull);
@@ -1395,7 +1458,12 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
     c.has_drift = true;
   }
   mark(c, kPhaseSearch);
-  const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches);
+  // The first search keeps its candidates, padded by kRecheckReach more than
+  // the candidate margin, for the overlap re-checks of the refinement rounds.
+  const bool keep = c.colonies == 0;
+  const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches,
+                                           keep ? p.candidate_margin + kRecheckReach : p.candidate_margin, keep);
+  if (!keep) c.kept_valid = false;
   mark(c, kPhaseRows);
   c.rows.count = 0;
   c.rows.ensure(std::max<std::uint32_t>(found, 1));
@@ -1454,9 +1522,10 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
     c.trial.ensure(n);
     reset_scalars(c);
     launch_move(n, c.base.view(), {c.resp_a.p, c.resp_b.p}, dt, c.trial.view(), c.scalars.p + kRotationBits,
-                c.scalars.p + kInvalid, c.scalars.p + kStatus, c.stream);
+                c.scalars.p + kInvalid, c.scalars.p + kStatus, c.stream, c.scalars.p + kDisplacementBits);
     read_scalars(c);
     attempt.rotation = bits_to_float(c.host_scalars[kRotationBits]);
+    c.displacement = bits_to_float(c.host_scalars[kDisplacementBits]);
     if (c.host_scalars[kInvalid] != 0) break;
     launch_restore(n, c.trial.view(), c.state.view(), c.scalars.p + kStatus, c.stream);
 
@@ -1635,7 +1704,7 @@ void load_system(Ctx& c, const msb_contact_system& s, const float* multipliers) 
   c.n = std::uint32_t(s.body_count);
   c.has_drift = false;
   for (std::uint64_t b = 0; b < s.body_count && !c.has_drift; ++b) {
-    for (float v : s.bodies[b].drift) c.has_drift = c.has_drift || v != 0.0f;
+    for (float v : s.bodies[b].drift) c.has_drift = c.has_drift || v != 0.0f || std::signbit(v);
   }
   const std::uint32_t rows = std::uint32_t(s.row_count);
   c.body_a.ensure(std::max<std::uint32_t>(c.n, 1));

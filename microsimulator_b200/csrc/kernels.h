@@ -103,6 +103,9 @@ struct ContactSearchParams {
   float margin;
   float sine_threshold;
   float epsilon;
+  // >= 0: the narrow phase first keeps only the pairs whose padded boxes
+  // at this margin overlap (candidates taken from a wider or earlier search).
+  float box_margin = -1.0f;
 };
 
 // Buckets to allocate for `cells` cells (dense limit or hashed table) + 1.

@@ -212,7 +212,7 @@ __device__ __forceinline__ bool rotate_axis_angle(F3 d, F3 rot, float max_rot, F
 
 __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt,
                             GeometryBuffers trial, std::uint32_t* rotation_bits, std::uint32_t* invalid,
-                            std::uint32_t* status) {
+                            std::uint32_t* status, std::uint32_t* displacement_bits) {
   for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const float4 va = response.a[s];
     const float4 vb = response.b[s];
@@ -238,8 +238,22 @@ __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArray
     }
     const float len = pl.w + va.w * dt;
     if (!finite3(pos) || !finite3(dir) || !isfinite(len) || len < 0.0f) atomicExch(invalid, 1u);
-    trial.pos_len[s] = make_float4(pos.x, pos.y, pos.z, len);
-    trial.dir_rad[s] = make_float4(dir.x, dir.y, dir.z, dr.w);
+    const float4 moved_pl = make_float4(pos.x, pos.y, pos.z, len);
+    const float4 moved_dr = make_float4(dir.x, dir.y, dir.z, dr.w);
+    trial.pos_len[s] = moved_pl;
+    trial.dir_rad[s] = moved_dr;
+    if (displacement_bits != nullptr) {
+      // How far any face of the cell's unpadded box moved, rounded up: the
+      // bound under which a re-check may reuse the substep's candidates.
+      double from[6], to[6];
+      padded_box(pl, dr, 0.0f, from);
+      padded_box(moved_pl, moved_dr, 0.0f, to);
+      double moved = 0.0;
+#pragma unroll
+      for (int k = 0; k < 6; ++k) moved = fmax(moved, fabs(to[k] - from[k]));
+      const float bound = isfinite(moved) ? __double2float_ru(moved) : __int_as_float(0x7F800000);
+      atomic_max_nonnegative(displacement_bits, bound);
+    }
   }
 }
 
@@ -543,10 +557,11 @@ void launch_memory_ids(std::uint32_t rows, const uint2* slots, const std::uint64
 }
 
 void launch_move(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt, GeometryBuffers trial,
-                 std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream) {
+                 std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream,
+                 std::uint32_t* displacement_bits) {
   if (n == 0) return;
   move_kernel<<<grid_for(n, kThreads), kThreads, 0, stream>>>(n, base, response, dt, trial, rotation_bits, invalid,
-                                                               status);
+                                                               status, displacement_bits);
   count_launch();
 }
 

@@ -90,8 +90,11 @@ void launch_memory_ids(std::uint32_t rows, const uint2* slots, const std::uint64
 
 // moved (contact_dynamics.cpp:311-356): trial geometry, largest rotation
 // (bits) and a validity flag (0 = valid).
+// With displacement_bits, also the largest distance any face of a cell's
+// unpadded FP64 box moved (float bits, rounded up).
 void launch_move(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt, GeometryBuffers trial,
-                 std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream);
+                 std::uint32_t* rotation_bits, std::uint32_t* invalid, std::uint32_t* status, cudaStream_t stream,
+                 std::uint32_t* displacement_bits = nullptr);
 // A response from a per-cell motion guess: guess[s] = (dx, dy, dtheta, _),
 // the displacement in the xy-plane and the turn about z over `step_dt`;
 // the elongation rate is each body's nominal rate.
