@@ -15,10 +15,12 @@ the tolerance.  Divisions are input preparation and run between steps.
   roofline  the BB iteration (body pass + row pass) of the last solved
          system, CUDA events on the backend's stream, against algorithmic
          bytes R*96 + N*128 per iteration
-  cpu_baseline  the reference CPU backend (compiled from its sources) on a
-         bounded sample of the same workload, all host threads
+  cpu_baseline  the reference CPU backend (compiled from its sources) on the
+         first timed steps of the same colony from the same state, about
+         15 s of stepping, all host threads
 
---impl reference prints the reference CPU backend's line on that sample.
+--impl reference prints the reference CPU backend's line for the same K
+timed steps from the same state.
 Multi-GPU: each rank steps its own independent colony (replicas; there is no
 data-path collective).
 """
@@ -52,8 +54,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cells", type=int, default=1_000_000)
-    p.add_argument("--cpu-cells", type=int, default=50_000)
-    p.add_argument("--cpu-seconds", type=float, default=12.0)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--seed", type=int, default=42)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
@@ -176,45 +177,82 @@ def ncu_traffic():
     return json.loads(path.read_text())
 
 
-def run_reference_sample(args, seconds, steps_cap, warm=2):
-    """The reference CPU backend on a bounded sample of the workload: `warm`
-    untimed steps (the overlap of the random start resolves in them), then
-    timed steps until `seconds` or `steps_cap`."""
-    from microsimulator_b200 import workloads
+def reference_steps(args, world, first_step, seconds, steps_cap, seed):
+    """The reference CPU backend (oracle/_ref, compiled from its sources)
+    stepping `world` through its own Simulation::step: the benchmark's
+    divisions before each step (steps first_step, first_step + 1, ...), timed
+    steps until `seconds` of stepping or `steps_cap` steps.  None without the
+    library."""
     from oracle.native import REFERENCE_PATH, Reference
 
     if not REFERENCE_PATH.exists():
         return None
     ref = Reference()
-    world = workloads.jammed(n=args.cpu_cells, seed=args.seed)
-    handle = ref.world_create(world)
+    plan_world = world.copy()
+    handle = ref.world_create(plan_world)
     try:
-        plan_world = world.copy()
-        for step in range(warm):
-            plan = divide(plan_world, step, args.seed)
-            ref.world_divide(handle, plan.parents, plan.rotations)
-            ref.world_step(handle, DT, dynamics())
-            ref.world_read(handle, plan_world)
-            plan_world.next_id = int(plan_world.ids.max()) + 1
-        cells_steps = 0
-        elapsed = 0.0
-        steps = 0
+        cells_steps, elapsed, steps, first_cells = 0, 0.0, 0, len(plan_world)
         while steps < steps_cap and (elapsed < seconds or steps == 0):
-            plan = divide(plan_world, steps + warm, args.seed)
+            plan = divide(plan_world, first_step + steps, seed)
             ref.world_divide(handle, plan.parents, plan.rotations)
+            n = len(plan_world)
             t0 = time.perf_counter()
             ref.world_step(handle, DT, dynamics())
             elapsed += time.perf_counter() - t0
-            cells_steps += len(plan_world)
+            cells_steps += n
             ref.world_read(handle, plan_world)
             plan_world.next_id = int(plan_world.ids.max()) + 1
             steps += 1
         return {"value": cells_steps / elapsed, "unit": "cell-steps/s", "cores": ref.thread_count(),
-                "kind": "reference",
-                "sample": f"{args.cpu_cells} capsules of the same distribution and area fraction, "
-                          f"{steps} timed steps after {warm} untimed, {elapsed:.1f} s"}
+                "kind": "reference", "steps": steps, "seconds": elapsed, "first_cells": first_cells,
+                "last_cells": len(plan_world)}
     finally:
         ref.world_destroy(handle)
+
+
+def warmed_colony(args, rank=0):
+    """The benchmark's colony after its --warmup steps: the jammed random
+    start with its divisions, stepped by the GPU stepper (by the reference
+    where no GPU is present).  The warm-up steps resolve the random start's
+    deep overlaps; on the reference CPU backend the first of them alone takes
+    many minutes at 1M capsules, so both arms take the state after them from
+    the GPU stepper (the same bits), and the reference's timed steps start
+    from it.  Returns the colony and what stepped the warm-up."""
+    import torch
+
+    from microsimulator_b200 import workloads
+
+    world = workloads.jammed(n=args.cells, seed=args.seed + rank)
+    if not torch.cuda.is_available():
+        from oracle.native import Reference
+
+        ref = Reference()
+        handle = ref.world_create(world)
+        try:
+            for step in range(args.warmup):
+                plan = divide(world, step, args.seed + rank)
+                ref.world_divide(handle, plan.parents, plan.rotations)
+                ref.world_step(handle, DT, dynamics())
+                ref.world_read(handle, world)
+                world.next_id = int(world.ids.max()) + 1
+        finally:
+            ref.world_destroy(handle)
+        return world, "the reference CPU backend (no GPU present)"
+    from microsimulator_b200.backend import B200Backend, DeviceCells
+
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    backend = B200Backend(local)
+    try:
+        for step in range(args.warmup):
+            divide(world, step, args.seed + rank)
+            cells = DeviceCells(world, device=f"cuda:{local}")
+            backend.advance_contact_dynamics_device(cells, None, DT, dynamics())
+            torch.cuda.synchronize()
+            cells.download(world)
+            world.next_id = int(world.ids.max()) + 1
+    finally:
+        backend.close()
+    return world, "the GPU stepper, as for the GPU arm"
 
 
 def config(args, world_size):
@@ -228,14 +266,26 @@ def config(args, world_size):
 
 
 def reference_arm(args):
+    """The reference CPU backend on this arm's workload: the 1M-capsule
+    colony's K timed steps (with the same divisions) from the state after the
+    warm-up steps, all host threads.  Stops early after 600 s of stepping and
+    says so in cpu_baseline.sample."""
     rank = int(os.environ.get("RANK", "0"))
     world_size = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
-    sample = run_reference_sample(args, seconds=1e9, steps_cap=max(1, args.steps), warm=max(2, args.warmup))
-    if sample is None:
+    from oracle.native import REFERENCE_PATH
+
+    if not REFERENCE_PATH.exists():
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmsref.so was not built"}))
         return
+    world, warm_by = warmed_colony(args)
+    sample = reference_steps(args, world, args.warmup, seconds=600.0, steps_cap=max(1, args.steps), seed=args.seed)
+    sample["sample"] = (f"the {args.cells}-capsule colony's timed steps {args.warmup}..{args.warmup + sample['steps'] - 1}"
+                        f" ({sample['first_cells']} -> {sample['last_cells']} capsules) from the state after "
+                        f"{args.warmup} warm-up steps (stepped by {warm_by}), {sample['seconds']:.1f} s of stepping")
+    for key in ("steps", "seconds", "first_cells", "last_cells"):
+        sample.pop(key)
     print(json.dumps({
         "impl": "reference",
         "metric": "cell-steps/s at 1M capsules, 1e-3 overlap tol",
@@ -517,6 +567,19 @@ def sweep_arm(args, backend, local, rank, dist):
     }
 
 
+def compact(arm):
+    """An arm's record without its workload text and per-phase breakdowns
+    (those go to stderr in full)."""
+    if arm is None:
+        return None
+    out = {}
+    for key, value in arm.items():
+        if key in ("workload", "phase_ms_per_step", "sharding", "sample", "how", "timing"):
+            continue
+        out[key] = compact(value) if isinstance(value, dict) else value
+    return out
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -662,9 +725,25 @@ def main():
 
     cpu = None
     if rank == 0 and world_size == 1 and not args.no_cpu:
-        cpu = run_reference_sample(args, seconds=args.cpu_seconds, steps_cap=50)
+        # The reference CPU backend on the first timed steps of the same
+        # colony from the same state (the snapshot after the warm-up).
+        cpu = reference_steps(args, snapshot, args.warmup, seconds=args.cpu_seconds, steps_cap=args.steps,
+                              seed=args.seed + rank)
+        if cpu is not None:
+            cpu["sample"] = (f"the first {cpu['steps']} timed steps of the same colony from the same state "
+                             f"({cpu['first_cells']} capsules), {cpu['seconds']:.1f} s of stepping")
+            for key in ("steps", "seconds", "first_cells", "last_cells"):
+                cpu.pop(key)
 
     if rank == 0:
+        # The arms' full records go to stderr, one JSON line each; the
+        # benchmark line keeps their headline figures.
+        for name, arm in (("learned", learned), ("sweep", sweep_line), ("walls", walls_line),
+                          ("contact_graph", graph_line)):
+            if arm is not None:
+                print(json.dumps({"arm": name, **arm}), file=sys.stderr)
+        learned, sweep_line, walls_line, graph_line = (compact(learned), compact(sweep_line), compact(walls_line),
+                                                       compact(graph_line))
         line = {
             "metric": "cell-steps/s at 1M capsules, 1e-3 overlap tol",
             "value": value,
