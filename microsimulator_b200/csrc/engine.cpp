@@ -127,6 +127,7 @@ struct RowStore {
   DBuf<std::uint64_t> partner;
   DBuf<float> multipliers;
   DBuf<float> gaps;
+  DBuf<float2> iterate;  // (multiplier, gap) inside a solve
   DBuf<std::uint32_t> keyed_offsets;
   DBuf<std::uint32_t> keyed_rows;
   std::uint32_t count = 0;
@@ -141,6 +142,7 @@ struct RowStore {
     partner.ensure(n);
     multipliers.ensure(n);
     gaps.ensure(n);
+    iterate.ensure(n);
   }
   void grow(std::size_t n, cudaStream_t s) {
     a.grow(n, count, s);
@@ -151,6 +153,7 @@ struct RowStore {
     partner.grow(n, count, s);
     multipliers.grow(n, count, s);
     gaps.grow(n, count, s);
+    iterate.ensure(n);  // filled by each solve
   }
   KeyedLists keyed() const { return {keyed_offsets.p, keyed_rows.p, partner.p, multipliers.p}; }
 };
@@ -1055,6 +1058,7 @@ void fill_desc(Ctx& c, std::uint32_t row_count, float dt, const msb_growth_load_
   d.response = {c.resp_a.p, c.resp_b.p};
   d.multipliers = c.rows.multipliers.p;
   d.gaps = c.rows.gaps.p;
+  d.iterate = c.rows.iterate.p;
   d.partials = c.partials.p;
   d.row_count = row_count;
   d.body_count = c.n;
@@ -1145,8 +1149,9 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
     fill_desc(c, rows, dt, growth, tolerance, max_iterations);
     check(cudaError_t(graph.launch(c.stream)), "solve launch");
   }
-  // The response of the final multipliers (the passes of a solve write only
-  // the rows' side terms).
+  // The final multipliers and gaps, and their response (the passes of a
+  // solve write only the rows' side terms).
+  launch_unpack_iterate(c.desc, c.last_blocks, c.stream);
   launch_evaluate(c.desc, c.last_blocks, false, c.stream);
   check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read desc");
   sync(c);

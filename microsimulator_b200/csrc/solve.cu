@@ -103,7 +103,7 @@ template <bool Coherent>
 __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
                                           std::uint32_t blocks, std::uint32_t* check) {
   const float* __restrict__ g = d.multipliers;
-  const float* __restrict__ gap = d.gaps;
+  const float2* __restrict__ iterate = d.iterate;
   const std::uint32_t* __restrict__ offsets = d.incidence.offsets;
   const float4* __restrict__ entry_a = d.incidence.a;
   const float4* __restrict__ entry_b = d.incidence.b;
@@ -134,8 +134,15 @@ __device__ __forceinline__ void body_pass(const SolveDesc& d, std::uint32_t mode
         if (k0 + t < end) {
           const std::uint32_t row = __float_as_uint(eb[t].w) >> 1;
           const bool ok = index_ok(row, d.row_count, check);
-          gv[t] = ok ? shared_load<Coherent>(&g[row]) : 0.0f;
-          pv[t] = ok && mode == 1 ? shared_load<Coherent>(&gap[row]) : 0.0f;
+          if (mode == 2) {
+            gv[t] = ok ? g[row] : 0.0f;
+            pv[t] = 0.0f;
+          } else {
+            // One gather brings the row's multiplier and gap.
+            const float2 q = ok ? shared_load<Coherent>(&iterate[row]) : make_float2(0.0f, 0.0f);
+            gv[t] = q.x;
+            pv[t] = mode == 1 ? q.y : 0.0f;
+          }
         }
       }
 #pragma unroll
@@ -198,8 +205,9 @@ template <bool Coherent>
 __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode, float alpha, std::uint32_t block,
                                          std::uint32_t blocks, std::uint32_t* check) {
   const float dt = d.dt;
-  float* __restrict__ g = d.multipliers;
+  const float* __restrict__ g = d.multipliers;
   float* __restrict__ gap = d.gaps;
+  float2* __restrict__ iterate = d.iterate;
   const float2* __restrict__ sides = d.incidence.sides;
   const float2* __restrict__ constants = d.incidence.constants;
   double ss = 0.0, sy = 0.0, yy = 0.0;
@@ -212,8 +220,10 @@ __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode,
   // x + -0.0f == x, so the sum is the reference's bit for bit.
   const bool project = mode == 1;
   for (std::uint32_t i = block * blockDim.x + threadIdx.x; i < d.row_count; i += blocks * blockDim.x) {
-    const float gi = shared_load<Coherent>(&g[i]);
-    const float gpi = project ? shared_load<Coherent>(&gap[i]) : 0.0f;
+    // mode 2 (an evaluation) reads the multipliers; a solve its iterate.
+    const float2 q = mode == 2 ? make_float2(g[i], 0.0f) : shared_load<Coherent>(&iterate[i]);
+    const float gi = q.x;
+    const float gpi = project ? q.y : 0.0f;
     const float2 side = shared_load<Coherent>(&sides[i]);
     const float2 k = __ldcs(&constants[i]);
     const float m = project ? smax(0.0f, gi - alpha * gpi) : gi;
@@ -227,9 +237,12 @@ __device__ __forceinline__ void row_pass(const SolveDesc& d, std::uint32_t mode,
       ss += moved * moved;
       sy += moved * change;
       yy += change * change;
-      g[i] = m;
     }
-    gap[i] = gn;
+    if (mode == 2) {
+      gap[i] = gn;
+    } else {
+      iterate[i] = make_float2(m, gn);
+    }
   }
   if (mode == 2) return;
 
@@ -359,6 +372,7 @@ __device__ __forceinline__ void bound_pass(const SolveDesc& d, std::uint32_t* bo
                                            std::uint32_t blocks) {
   float bound = 0.0f;
   for (std::uint32_t i = block * blockDim.x + threadIdx.x; i < d.row_count; i += blocks * blockDim.x) {
+    d.iterate[i] = make_float2(d.multipliers[i], 0.0f);
     const uint2 s = d.rows.slots[i];
     const float4 ra = d.rows.a[i];
     const float4 rb = d.rows.b[i];
@@ -448,6 +462,7 @@ __global__ void __launch_bounds__(kSolveThreads) bound_kernel(SolveDesc* desc) {
   SolveDesc& d = *desc;
   float bound = 0.0f;
   for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
+    d.iterate[i] = make_float2(d.multipliers[i], 0.0f);  // the solve's starting multipliers
     const uint2 s = d.rows.slots[i];
     const float4 ra = d.rows.a[i];
     const float4 rb = d.rows.b[i];
@@ -459,6 +474,15 @@ __global__ void __launch_bounds__(kSolveThreads) bound_kernel(SolveDesc* desc) {
   for (int o = 16; o > 0; o >>= 1) bound = smax(bound, __shfl_down_sync(0xFFFFFFFFu, bound, o));
   // Non-negative floats order as their bit patterns.
   if ((threadIdx.x & 31) == 0 && bound > 0.0f) atomicMax(&d.bound_bits, __float_as_uint(bound));
+}
+
+__global__ void unpack_iterate_kernel(const SolveDesc* desc) {
+  const SolveDesc& d = *desc;
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < d.row_count; i += gridDim.x * blockDim.x) {
+    const float2 q = d.iterate[i];
+    d.multipliers[i] = q.x;
+    d.gaps[i] = q.y;
+  }
 }
 
 __global__ void solve_reset_kernel(SolveDesc* desc) {
@@ -778,6 +802,11 @@ void launch_iteration(SolveDesc* desc, int blocks, cudaEvent_t between, cudaStre
   if (between != nullptr) cudaEventRecord(between, stream);
   row_pass_kernel<1><<<blocks, kSolveThreads, 0, stream>>>(desc, 1, 0);
   count_launch(2);
+}
+
+void launch_unpack_iterate(SolveDesc* desc, int blocks, cudaStream_t stream) {
+  unpack_iterate_kernel<<<blocks, kSolveThreads, 0, stream>>>(desc);
+  count_launch();
 }
 
 void launch_evaluate(SolveDesc* desc, int blocks, bool with_gaps, cudaStream_t stream) {

@@ -65,6 +65,10 @@ struct SolveDesc {
   ResponseArrays response;
   float* multipliers;
   float* gaps;
+  // (multiplier, gap) of every row while a solve runs: the body pass
+  // gathers both with one load.  The bound pass fills it from `multipliers`;
+  // launch_unpack_iterate writes the solution back.
+  float2* iterate;
   double* partials;  // 5 doubles per block of the row pass
   std::uint32_t row_count;
   std::uint32_t body_count;
@@ -149,6 +153,9 @@ constexpr unsigned long long kBarrierTimeoutNs = 5'000'000'000ull;
 // writes no response itself: this evaluation of its final multipliers
 // follows it.
 void launch_evaluate(SolveDesc* desc, int blocks, bool with_gaps, cudaStream_t stream);
+// The multipliers and gaps a solve reached (desc->iterate) into
+// desc->multipliers and desc->gaps.
+void launch_unpack_iterate(SolveDesc* desc, int blocks, cudaStream_t stream);
 
 // One more projected iteration of the last solved system (body pass then
 // row pass), for timing; `between` is recorded between the two passes.
