@@ -1409,7 +1409,7 @@ void learned_guess(Ctx& c, float dt) {
   c.net_outputs.ensure(3ull * std::max<std::uint32_t>(n, 1));
   c.guess.ensure(std::max<std::uint32_t>(n, 1));
   check(cudaError_t(mlp::launch_forward_tc(c.net_weights.p, c.net_biases.p, c.features.p, n, c.net_outputs.p,
-                                           c.scalars.p + kStatus, c.stream)),
+                                           nullptr, c.scalars.p + kStatus, c.stream)),
         "warm-start network");
   mlp::launch_outputs_to_guess(n, c.net_outputs.p, c.net_scale, c.state.dir_rad.p, c.guess.p, c.stream);
   check(cudaGetLastError(), "warm-start network");
@@ -2029,14 +2029,9 @@ int msb_mlp_forward(const uint16_t* weights, const float* biases, const uint16_t
   if (rows > 0 && (weights == nullptr || biases == nullptr || features == nullptr || outputs == nullptr)) {
     return MSB_ERR_INVALID_ARGUMENT;
   }
-  if (activations == nullptr) {
-    // Inference: the tcgen05 pass.
-    return cuda_status(cudaError_t(mlp::launch_forward_tc(weights, biases, features, std::uint32_t(rows), outputs,
-                                                          nullptr, static_cast<cudaStream_t>(stream))));
-  }
-  mlp::launch_forward(weights, biases, features, std::uint32_t(rows), outputs, activations,
-                      static_cast<cudaStream_t>(stream));
-  return cuda_status(cudaGetLastError());
+  // The tcgen05 pass, keeping the activations for training when given them.
+  return cuda_status(cudaError_t(mlp::launch_forward_tc(weights, biases, features, std::uint32_t(rows), outputs,
+                                                        activations, nullptr, static_cast<cudaStream_t>(stream))));
 }
 
 int msb_mlp_backward(const uint16_t* weights, const uint16_t* features, uint64_t rows, const void* activations,
@@ -2047,9 +2042,8 @@ int msb_mlp_backward(const uint16_t* weights, const uint16_t* features, uint64_t
                    scratch == nullptr)) {
     return MSB_ERR_INVALID_ARGUMENT;
   }
-  mlp::launch_backward(weights, features, std::uint32_t(rows), activations, output_grad, grads, scratch,
-                       static_cast<cudaStream_t>(stream));
-  return cuda_status(cudaGetLastError());
+  return cuda_status(cudaError_t(mlp::launch_backward(weights, features, std::uint32_t(rows), activations, output_grad,
+                                                      grads, scratch, nullptr, static_cast<cudaStream_t>(stream))));
 }
 
 int msb_mlp_adam(float* params, const float* grads, float* m, float* v, uint32_t step, float lr, float beta1,

@@ -1,6 +1,7 @@
-// The warm-start network's inference pass on the fifth-generation tensor
-// cores: tcgen05.mma with both operands in shared memory and the fp32
-// accumulator in tensor memory (TMEM).
+// The warm-start network on the fifth-generation tensor cores: tcgen05.mma
+// with both operands in shared memory and the fp32 accumulator in tensor
+// memory (TMEM), for the forward pass (inference, and training with its
+// activations kept) and for the backward pass's GEMMs.
 //
 // One CTA of 512 threads per SM works through 128-cell tiles.  Per layer:
 // thread 0 issues the layer's K/16 MMAs (M = 128 cells, N = 128 outputs, or 16
@@ -17,6 +18,7 @@
 // K blocks R/8 * 128 bytes apart (its leading byte offset) for R rows.
 #include <cuda_bf16.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "device.cuh"
@@ -144,7 +146,8 @@ __device__ void stage_weights(unsigned char* smem, const std::uint16_t* w, std::
 __global__ void __launch_bounds__(kTcThreads, 1) forward_tc_kernel(const std::uint16_t* __restrict__ weights,
                                                               const float* __restrict__ biases,
                                                               const std::uint16_t* __restrict__ x, std::uint32_t n,
-                                                              float* __restrict__ y, std::uint32_t* error) {
+                                                              float* __restrict__ y, Activations act, int keep,
+                                                              std::uint32_t* error) {
   extern __shared__ __align__(128) unsigned char smem[];
   const std::uint32_t base = static_cast<std::uint32_t>(__cvta_generic_to_shared(smem));
   const std::uint32_t barrier = base + kOffBarrier;
@@ -229,12 +232,22 @@ __global__ void __launch_bounds__(kTcThreads, 1) forward_tc_kernel(const std::ui
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const std::uint32_t k0 = c * 32 + q * 8;
+            float z[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) z[j] = v[q * 8 + j] + b[k0 + j];
             uint4 out;
-            out.x = pack(gelu(v[q * 8 + 0] + b[k0 + 0]), gelu(v[q * 8 + 1] + b[k0 + 1]));
-            out.y = pack(gelu(v[q * 8 + 2] + b[k0 + 2]), gelu(v[q * 8 + 3] + b[k0 + 3]));
-            out.z = pack(gelu(v[q * 8 + 4] + b[k0 + 4]), gelu(v[q * 8 + 5] + b[k0 + 5]));
-            out.w = pack(gelu(v[q * 8 + 6] + b[k0 + 6]), gelu(v[q * 8 + 7] + b[k0 + 7]));
+            out.x = pack(gelu(z[0]), gelu(z[1]));
+            out.y = pack(gelu(z[2]), gelu(z[3]));
+            out.z = pack(gelu(z[4]), gelu(z[5]));
+            out.w = pack(gelu(z[6]), gelu(z[7]));
             *reinterpret_cast<uint4*>(a + core_offset(kTile, row, k0)) = out;
+            if (keep && cell < n) {
+              // Training: this layer's pre-activations and activations for the backward pass.
+              float* zr = act.z[layer] + std::size_t(cell) * kHidden + k0;
+              *reinterpret_cast<float4*>(zr) = make_float4(z[0], z[1], z[2], z[3]);
+              *reinterpret_cast<float4*>(zr + 4) = make_float4(z[4], z[5], z[6], z[7]);
+              *reinterpret_cast<uint4*>(act.h[layer] + std::size_t(cell) * kHidden + k0) = out;
+            }
           }
         }
       } else if (chunk == 0) {
@@ -256,10 +269,172 @@ __global__ void __launch_bounds__(kTcThreads, 1) forward_tc_kernel(const std::ui
   }
 }
 
+// ------------------------------------------------------------- the GEMM
+//
+// C (m x n) = A (m x k) B (k x n), bf16 operands through element strides.
+// A CTA computes a 128-row tile of C (rows past m zero) over its share of k
+// (grid z splits k): per 64-wide k chunk its 128 threads stage the A chunk
+// (128 x 64) and the B chunk (n rounded up to 16, x 64) in the canonical
+// K-major layout, thread 0 issues four tcgen05.mma (K = 16 each) into the
+// TMEM accumulator and commits them to an mbarrier, and the chunk after
+// waits for them.  The four warps then read their 32 lanes of the
+// accumulator with tcgen05.ld and store C (or the split's partial sums).
+
+constexpr int kGemmThreads = 128;
+constexpr std::uint32_t kGemmChunk = 64;
+constexpr std::uint32_t kGemmMaxSplits = 32;
+constexpr std::uint32_t kGemmBytesA = 128 * kGemmChunk * 2;  // 16 KB
+constexpr std::uint32_t kGemmBytesB = 128 * kGemmChunk * 2;  // 16 KB (n <= 128)
+constexpr std::uint32_t kGemmOffB = kGemmBytesA;
+constexpr std::uint32_t kGemmOffBarrier = kGemmOffB + kGemmBytesB;
+constexpr std::uint32_t kGemmOffTmem = kGemmOffBarrier + 8;
+// More shared memory than the operands need, so that at most four CTAs
+// share an SM: four 128-column accumulators fill its 512 TMEM columns.
+constexpr std::size_t kGemmSmem = 56 * 1024;
+static_assert(kGemmOffTmem + 8 <= kGemmSmem, "gemm shared memory");
+
+__global__ void __launch_bounds__(kGemmThreads) gemm_tc_kernel(Gemm p, std::uint32_t chunk_split, float* partials,
+                                                              std::uint32_t* error) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  const std::uint32_t base = static_cast<std::uint32_t>(__cvta_generic_to_shared(smem));
+  const std::uint32_t barrier = base + kGemmOffBarrier;
+  std::uint32_t* tmem_slot = reinterpret_cast<std::uint32_t*>(smem + kGemmOffTmem);
+  __shared__ int ok;
+  const std::uint32_t nt = (p.n + 15) / 16 * 16;  // the MMA's N
+  const std::uint32_t m0 = blockIdx.y * 128;
+  const std::uint32_t k_begin = blockIdx.z * chunk_split * kGemmChunk;
+  const std::uint32_t k_end = smin<std::uint32_t>(p.k, k_begin + chunk_split * kGemmChunk);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(barrier), "r"(1u) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    ok = 1;
+  }
+  if (threadIdx.x < 32) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(base + kGemmOffTmem),
+                 "r"(kTmemColumns)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_before();
+  __syncthreads();
+  fence_after();
+  const std::uint32_t tmem = *tmem_slot;
+  unsigned char* sa = smem;
+  unsigned char* sb = smem + kGemmOffB;
+  std::uint32_t phase = 0;
+  std::uint32_t issued = 0;
+  for (std::uint32_t k0 = k_begin; k0 < k_end; k0 += kGemmChunk) {
+    // Stage the chunk: A (128 x 64) and B (nt x 64), zero outside the matrices.
+    for (std::uint32_t e = threadIdx.x; e < 128 * kGemmChunk; e += kGemmThreads) {
+      const std::uint32_t r = e / kGemmChunk, kk = e % kGemmChunk;
+      const std::uint32_t mm = m0 + r, k = k0 + kk;
+      const std::uint16_t va = (mm < p.m && k < k_end) ? p.a[std::int64_t(mm) * p.sam + std::int64_t(k) * p.sak] : 0;
+      *reinterpret_cast<std::uint16_t*>(sa + core_offset(128, r, kk)) = va;
+      if (r < nt) {
+        const std::uint16_t vb = (r < p.n && k < k_end) ? p.b[std::int64_t(k) * p.sbk + std::int64_t(r) * p.sbn] : 0;
+        *reinterpret_cast<std::uint16_t*>(sb + core_offset(nt, r, kk)) = vb;
+      }
+    }
+    fence_async_smem();
+    fence_before();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      fence_after();
+      const std::uint32_t idesc = instr_descriptor(nt);
+      for (std::uint32_t s = 0; s < kGemmChunk / 16; ++s) {
+        const std::uint64_t ad = smem_descriptor(base + 2 * s * (128 / 8) * 128, (128 / 8) * 128, 128);
+        const std::uint64_t bd = smem_descriptor(base + kGemmOffB + 2 * s * (nt / 8) * 128, (nt / 8) * 128, 128);
+        mma(tmem, ad, bd, idesc, (issued > 0 || s > 0) ? 1u : 0u);
+      }
+      commit(barrier);
+      std::uint32_t polls = 0;
+      while (!try_wait(barrier, phase)) {
+        if (++polls > kWaitPolls) {
+          ok = 0;
+          if (error != nullptr) atomicExch(error, std::uint32_t(kStatusIterations));
+          break;
+        }
+      }
+    }
+    phase ^= 1u;
+    ++issued;
+    __syncthreads();
+    if (!ok) break;
+  }
+  fence_after();
+  // Epilogue: warp w holds rows 32w..32w+31 of the tile, one per lane.
+  const std::uint32_t warp = threadIdx.x >> 5;
+  const std::uint32_t row = m0 + warp * 32 + (threadIdx.x & 31);
+  if (ok) {
+    for (std::uint32_t c0 = 0; c0 < nt; c0 += 32) {
+      float v[32];
+      if (issued > 0) {
+        load32(tmem + ((warp * 32u) << 16) + c0, v);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 32; ++j) v[j] = 0.0f;  // an empty share of k
+      }
+      if (row < p.m) {
+        for (std::uint32_t j = 0; j < 32 && c0 + j < p.n; ++j) {
+          const std::uint32_t col = c0 + j;
+          if (partials != nullptr) {
+            partials[(std::size_t(blockIdx.z) * p.m + row) * p.n + col] = v[j];
+          } else {
+            p.c[std::int64_t(row) * p.scm + std::int64_t(col) * p.scn] = v[j];
+          }
+        }
+      }
+    }
+  }
+  fence_before();
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemColumns) : "memory");
+  }
+}
+
+// C = the sum of the splits' partial sums, in split order.
+__global__ void gemm_reduce_kernel(Gemm p, std::uint32_t splits, const float* __restrict__ partials) {
+  const std::uint64_t total = std::uint64_t(p.m) * p.n;
+  for (std::uint64_t i = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; i < total;
+       i += std::uint64_t(gridDim.x) * blockDim.x) {
+    float sum = 0.0f;
+    for (std::uint32_t z = 0; z < splits; ++z) sum += partials[z * total + i];
+    const std::uint32_t row = std::uint32_t(i / p.n), col = std::uint32_t(i % p.n);
+    p.c[std::int64_t(row) * p.scm + std::int64_t(col) * p.scn] = sum;
+  }
+}
+
 }  // namespace
 
+int tc_gemm(const Gemm& p, float* partials, std::uint32_t* error, cudaStream_t stream) {
+  if (p.m == 0 || p.n == 0) return 0;
+  if (p.n > 128) return int(cudaErrorInvalidValue);
+  cudaError_t e = cudaFuncSetAttribute(gemm_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kGemmSmem));
+  if (e != cudaSuccess) return int(e);
+  const std::uint32_t tiles = (p.m + 127) / 128;
+  const std::uint32_t chunks = std::max<std::uint32_t>(1, (p.k + kGemmChunk - 1) / kGemmChunk);
+  // A long k over several CTAs when the tiles alone leave SMs idle.
+  std::uint32_t splits = 1;
+  if (tiles < 64 && partials != nullptr && std::uint64_t(p.m) * p.n * kGemmMaxSplits * 4 <= kGemmPartialBytes) {
+    splits = std::min(std::min(kGemmMaxSplits, chunks), std::max<std::uint32_t>(1, 128 / tiles));
+  }
+  const std::uint32_t per_split = (chunks + splits - 1) / splits;
+  splits = (chunks + per_split - 1) / per_split;
+  const dim3 grid(1, tiles, splits);
+  gemm_tc_kernel<<<grid, kGemmThreads, kGemmSmem, stream>>>(p, per_split, splits > 1 ? partials : nullptr, error);
+  count_launch();
+  if (splits > 1) {
+    gemm_reduce_kernel<<<grid_for(std::uint64_t(p.m) * p.n, 256), 256, 0, stream>>>(p, splits, partials);
+    count_launch();
+  }
+  return int(cudaGetLastError());
+}
+
 int launch_forward_tc(const std::uint16_t* weights, const float* biases, const std::uint16_t* features,
-                      std::uint32_t n, float* outputs, std::uint32_t* error, cudaStream_t stream) {
+                      std::uint32_t n, float* outputs, void* activations, std::uint32_t* error,
+                      cudaStream_t stream) {
   if (n == 0) return 0;
   cudaError_t e = cudaFuncSetAttribute(forward_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmem));
   if (e != cudaSuccess) return int(e);
@@ -268,7 +443,9 @@ int launch_forward_tc(const std::uint16_t* weights, const float* biases, const s
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
   const std::uint32_t tiles = (n + kTile - 1) / kTile;
   const std::uint32_t blocks = std::max(1u, std::min<std::uint32_t>(tiles, std::uint32_t(sms)));
-  forward_tc_kernel<<<blocks, kTcThreads, kTcSmem, stream>>>(weights, biases, features, n, outputs, error);
+  const Activations act = activations != nullptr ? activations_at(activations, n) : Activations{};
+  forward_tc_kernel<<<blocks, kTcThreads, kTcSmem, stream>>>(weights, biases, features, n, outputs, act,
+                                                             activations != nullptr ? 1 : 0, error);
   count_launch();
   return int(cudaGetLastError());
 }

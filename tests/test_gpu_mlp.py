@@ -1,7 +1,7 @@
 """The warm-start network's kernels through the C-ABI against the numpy
-oracle (oracle/mlp_oracle.py): features bit for bit, the tensor-core
-forward and backward within bf16 tolerances, Adam, training, and the learned
-warm start in the stepper."""
+oracle (oracle/mlp_oracle.py): features bit for bit, the tcgen05 forward
+(inference and training) and backward within bf16 tolerances, Adam,
+training, and the learned warm start in the stepper."""
 
 import numpy as np
 import pytest
@@ -67,24 +67,46 @@ def test_forward_matches_oracle(backend):
     assert np.array_equal(y7, y[:7])
 
 
-def test_tcgen05_inference_matches_the_training_forward(backend):
-    """The inference pass (tcgen05, TMEM accumulators) and the training
-    pass (mma.sync) compute the same network: equal up to the order of the
-    fp32 sums inside the tensor cores and the bf16 roundings that follow."""
+def activations_of(act, n):
+    """H1..H3 (bf16) and Z1..Z3 (fp32) from the buffer the training forward keeps."""
+    raw = act.cpu().numpy()
+    h_bytes, z_bytes = n * mo.HIDDEN * 2, n * mo.HIDDEN * 4
+    h = [mo.from_bf16_bits(raw[l * h_bytes:(l + 1) * h_bytes].view(np.uint16).reshape(n, mo.HIDDEN)) for l in range(3)]
+    base = 3 * h_bytes
+    z = [raw[base + l * z_bytes:base + (l + 1) * z_bytes].view(np.float32).reshape(n, mo.HIDDEN) for l in range(3)]
+    return h, z
+
+
+def test_training_forward_on_tcgen05_matches_inference_and_the_oracle(backend):
+    """Training and inference run the same tcgen05 kernel (TMEM
+    accumulators): the outputs are the same bits with and without kept
+    activations, and the kept pre-activations Z and activations H match the
+    numpy oracle's, across tile edges (1, 127, 128, 129 rows) and a larger
+    batch."""
     net, p = network(4, backend._lib)
     for n in (1, 127, 128, 129, 5000):
-        x = bf16_tensor(random_batch(n, 40 + n))
+        xn = random_batch(n, 40 + n)
+        x = bf16_tensor(xn)
         infer = net.forward(x).cpu().numpy()
-        train, _ = net.forward(x, keep=True)
-        train = train.cpu().numpy()
-        scale = max(np.abs(train).max(), 1e-6)
-        assert np.max(np.abs(infer - train)) <= 1e-2 * scale, (n, np.max(np.abs(infer - train)) / scale)
-        assert np.all(np.isfinite(infer))
+        train, act = net.forward(x, keep=True)
+        assert np.array_equal(train.cpu().numpy(), infer), n
+        ref, cache = mo.forward(p, xn, round_like_kernels=True)
+        scale = max(np.abs(ref).max(), 1e-6)
+        assert np.max(np.abs(infer - ref)) <= 1e-2 * scale, (n, np.max(np.abs(infer - ref)) / scale)
+        h, z = activations_of(act, n)
+        for layer in range(3):
+            zs = max(np.abs(cache["z"][layer]).max(), 1e-6)
+            assert np.max(np.abs(z[layer] - cache["z"][layer])) <= 1e-2 * zs, (n, layer)
+            hs = max(np.abs(cache["h"][layer + 1]).max(), 1e-6)
+            assert np.max(np.abs(h[layer] - cache["h"][layer + 1])) <= 2e-2 * hs, (n, layer)
 
 
-def test_backward_matches_oracle_gradient(backend):
+@pytest.mark.parametrize("n", [777, 20000])
+def test_backward_matches_oracle_gradient(backend, n):
+    """The backward GEMMs on tcgen05 (a long k split over several CTAs whose
+    partial sums are added in a fixed order at 20,000 rows) against the
+    oracle's FP64 gradient."""
     net, p = network(3, backend._lib)
-    n = 777
     x = random_batch(n, 4)
     rng = np.random.default_rng(5)
     dy = rng.normal(0, 1, (n, mo.OUTPUTS)).astype(np.float32) / n
