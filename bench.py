@@ -167,10 +167,10 @@ def measured_peak():
 
 def ncu_traffic():
     """DRAM bytes of one BB iteration as a multiple of its algorithmic bytes,
-    from the committed ncu capture (profiles/bb_iteration_traffic.json, a
-    500,000-capsule system); None without one.  The bench scales it to its own
-    launch by the algorithmic bytes, which grow with rows and bodies as the
-    traffic does."""
+    from the committed ncu capture (profiles/bb_iteration_traffic.json, the
+    1M-capsule colony's system after 2 steps: 2.2M rows, 1.04M bodies); None
+    without one.  The bench scales it to its own launches by the algorithmic
+    bytes, which grow with rows and bodies as the traffic does."""
     path = ROOT / "profiles" / "bb_iteration_traffic.json"
     if not path.exists():
         return None

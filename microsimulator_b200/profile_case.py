@@ -13,6 +13,11 @@ colony (``features_kernel``, ``forward_kernel``), timed with CUDA events:
 
   python -m microsimulator_b200.profile_case --case mlp --cells 1000000
 
+--case train: training steps of the warm-start network (``forward_tc_kernel``
+keeping activations, ``gemm_tc_kernel``, ``gemm_reduce_kernel``):
+
+  python -m microsimulator_b200.profile_case --case train --cells 8192 --iterations 5
+
 --case batch: one step of a batch of sweep colonies (``batch_solve_kernel``;
 the first call's autotuner launches the kernel once per launch shape first):
 
@@ -69,6 +74,40 @@ def mlp_case(args) -> None:
     best = min(times["forward_ms"])
     print(json.dumps({**times, "cells": args.cells, "forward_flops": flops,
                       "forward_tflops": flops / (best * 1e-3) / 1e12}))
+    backend.close()
+
+
+def train_case(args) -> None:
+    """Training steps of the warm-start network on random bf16 features: the
+    tcgen05 forward keeping its activations, the backward pass's tcgen05
+    GEMMs (split-K at this batch size) and Adam, --iterations steps of a
+    batch of --cells rows, timed with CUDA events."""
+    import torch
+
+    from . import learned
+    from .backend import B200Backend
+
+    backend = B200Backend(0)
+    net = learned.WarmStartNetwork("cuda:0", seed=args.seed, library=backend._lib)
+    gen = torch.Generator(device="cuda:0").manual_seed(args.seed)
+    x = torch.randn((args.cells, 96), device="cuda:0", generator=gen).to(torch.bfloat16).view(torch.int16)
+    x[:, 81:] = 0
+    target = torch.randn((args.cells, 3), device="cuda:0", generator=gen)
+    times = []
+    for _ in range(args.iterations):
+        s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s0.record()
+        out, act = net.forward(x, keep=True)
+        diff, factor = net.loss_and_grad(out, target)
+        net.backward(x, act, (diff * factor).contiguous())
+        net.adam(1e-3)
+        s1.record()
+        torch.cuda.synchronize()
+        times.append(s0.elapsed_time(s1))
+    # forward 2*n*(96*128 + 2*128*128 + 8*128); backward about twice that
+    flops = 3 * 2.0 * args.cells * (96 * 128 + 2 * 128 * 128 + 8 * 128)
+    print(json.dumps({"step_ms": times, "rows": args.cells, "approx_flops": flops,
+                      "approx_tflops": flops / (min(times) * 1e-3) / 1e12}))
     backend.close()
 
 
@@ -228,7 +267,7 @@ def trap_case(args) -> None:
 
 def main() -> None:
     p = argparse.ArgumentParser()
-    p.add_argument("--case", default="bb", choices=["bb", "mlp", "batch", "guess", "graph", "trap"])
+    p.add_argument("--case", default="bb", choices=["bb", "mlp", "train", "batch", "guess", "graph", "trap"])
     p.add_argument("--warm", type=int, default=3)
     p.add_argument("--colonies", type=int, default=64)
     p.add_argument("--cells", type=int, default=500_000)
@@ -238,6 +277,9 @@ def main() -> None:
     args = p.parse_args()
     if args.case == "mlp":
         mlp_case(args)
+        return
+    if args.case == "train":
+        train_case(args)
         return
     if args.case == "batch":
         batch_case(args)
