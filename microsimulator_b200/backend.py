@@ -383,17 +383,27 @@ class B200Backend:
                                  dynamics: ContactDynamicsParameters | None = None,
                                  contacts: ContactParameters | None = None,
                                  constraint_parameters: ConstraintContactParameters | None = None,
-                                 ) -> ContactDynamicsResult:
+                                 outputs=None) -> ContactDynamicsResult:
         """One contact-dynamics step of ``world`` (updated in place) with
-        host buffers: the upload, the step and the download in one call."""
+        host buffers: the upload, the step and the download in one call.
+        ``world`` is a WorldState or any object with its arrays (such as
+        PinnedCells, whose page-locked arrays the library copies without
+        staging).  ``outputs`` (velocities n x 3, loads n, increments n,
+        float32) receives the step's outputs; new arrays without it."""
         dynamics = dynamics or ContactDynamicsParameters()
         contacts = contacts or ContactParameters()
         constraint_parameters = constraint_parameters or ConstraintContactParameters()
         n = len(world)
         cells = world.arrays()
-        velocities = np.zeros((n, 3), dtype=np.float32)
-        loads = np.zeros(n, dtype=np.float32)
-        increments = np.zeros(n, dtype=np.float32)
+        if outputs is None:
+            velocities = np.zeros((n, 3), dtype=np.float32)
+            loads = np.zeros(n, dtype=np.float32)
+            increments = np.zeros(n, dtype=np.float32)
+        else:
+            velocities, loads, increments = outputs
+            for array, shape in ((velocities, (n, 3)), (loads, (n,)), (increments, (n,))):
+                if array.dtype != np.float32 or array.shape != shape or not array.flags.c_contiguous:
+                    raise ValueError("outputs must be C-contiguous float32 arrays of shapes (n, 3), (n,), (n,)")
         outputs = abi.ContactDynamicsOutputs(abi.ptr(velocities), abi.ptr(loads), abi.ptr(increments))
         report = abi.ContactDynamicsReport()
         dyn, cp, wp = dynamics.native(), contacts.native(), constraint_parameters.native()
@@ -499,6 +509,63 @@ class DeviceCells:
         for name in ("position_x", "position_y", "position_z", "direction_x", "direction_y", "direction_z",
                      "lengths"):
             setattr(world, name, self.fields[name].cpu().numpy().copy())
+
+
+class PinnedCells:
+    """A world's arrays in page-locked host memory (pinned torch tensors
+    viewed as numpy arrays), which the host-buffer calls copy to and from the
+    device directly.  ``load`` copies a WorldState in, ``store`` copies the
+    stepped geometry back; ``outputs`` are pinned output arrays for
+    ``advance_contact_dynamics(..., outputs=...)``."""
+
+    FIELDS = ("position_x", "position_y", "position_z", "direction_x", "direction_y", "direction_z", "lengths",
+              "radii", "growth_rates")
+
+    def __init__(self, capacity: int):
+        import torch
+
+        def pinned(count, dtype):
+            return torch.empty(count, dtype=dtype, pin_memory=True).numpy()
+
+        self.capacity = int(capacity)
+        self.count = 0
+        self._ids = pinned(self.capacity, torch.int64).view(np.uint64)
+        self._fields = {name: pinned(self.capacity, torch.float32) for name in self.FIELDS}
+        self._fixed = pinned(self.capacity, torch.uint8)
+        self._velocities = pinned(3 * self.capacity, torch.float32)
+        self._loads = pinned(self.capacity, torch.float32)
+        self._increments = pinned(self.capacity, torch.float32)
+
+    def __len__(self) -> int:
+        return self.count
+
+    def load(self, world) -> None:
+        n = len(world)
+        if n > self.capacity:
+            raise ValueError(f"{n} cells exceed the pinned capacity {self.capacity}")
+        self.count = n
+        self._ids[:n] = world.ids
+        for name in self.FIELDS:
+            self._fields[name][:n] = getattr(world, name)
+        self._fixed[:n] = world.fixed
+
+    def store(self, world) -> None:
+        n = self.count
+        for name in ("position_x", "position_y", "position_z", "direction_x", "direction_y", "direction_z",
+                     "lengths"):
+            setattr(world, name, self._fields[name][:n].copy())
+
+    def outputs(self):
+        n = self.count
+        return self._velocities[:3 * n].reshape(n, 3), self._loads[:n], self._increments[:n]
+
+    def arrays(self) -> abi.CellArrays:
+        f = self._fields
+        return abi.CellArrays(
+            self.count, abi.ptr(self._ids), abi.ptr(f["position_x"]), abi.ptr(f["position_y"]),
+            abi.ptr(f["position_z"]), abi.ptr(f["direction_x"]), abi.ptr(f["direction_y"]),
+            abi.ptr(f["direction_z"]), abi.ptr(f["lengths"]), abi.ptr(f["radii"]), abi.ptr(f["growth_rates"]),
+            abi.ptr(self._fixed))
 
 
 class DeviceOutputs:

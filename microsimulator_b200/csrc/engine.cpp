@@ -689,10 +689,27 @@ msb::HostCopies& host_copies(Ctx& c) {
   return *c.copies;
 }
 
-// A device-to-host copy into the caller's pageable `dst` through the pinned
-// download buffer: the DMA is queued now, the host copy waits in c.pending
-// for the stream's next sync (flush_downloads).  `at` is the running offset.
+// Whether `p` is page-locked host memory the device can reach by DMA
+// (cudaHostAlloc / cudaHostRegister / a pinned torch tensor): such caller
+// arrays are copied directly, without the staging buffers.
+bool pinned_host(const void* p) {
+  cudaPointerAttributes a{};
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeHost;
+}
+
+// A device-to-host copy into the caller's `dst`: directly when `dst` is
+// pinned, else through the pinned download buffer (the DMA is queued now,
+// the host copy waits in c.pending for the stream's next sync,
+// flush_downloads).  `at` is the running offset in the download buffer.
 void stage_download(Ctx& c, void* dst, const void* device_src, std::size_t bytes, std::size_t& at) {
+  if (pinned_host(dst)) {
+    check(cudaMemcpyAsync(dst, device_src, bytes, cudaMemcpyDeviceToHost, c.stream), "copy back");
+    return;
+  }
   unsigned char* slot = c.download.p + at;
   check(cudaMemcpyAsync(slot, device_src, bytes, cudaMemcpyDeviceToHost, c.stream), "copy back");
   // The host copy of this array may start once its own DMA is done.
@@ -751,18 +768,29 @@ void load_cells(Ctx& c, const msb_cell_arrays& cells, bool device_pointers) {
       check(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyDeviceToDevice, c.stream), "copy cells");
     }
   } else {
+    // Pinned caller arrays go straight to the device; the others through
+    // pinned staging: the host side in parallel, each 2 MiB chunk's DMA
+    // queued as soon as it is staged.
+    std::vector<msb::HostCopies::Job> pageable;
     std::size_t total = 0;
-    for (const auto& u : uploads) total += (u.bytes + 255) & ~std::size_t(255);
-    // Through pinned staging: the host side in parallel, each 2 MiB chunk's
-    // DMA queued as soon as it is staged.
-    unsigned char* base = c.upload.ensure(total);
-    std::vector<msb::HostCopies::Job> host;
-    std::size_t at = 0;
     for (const auto& u : uploads) {
-      host.push_back({base + at, u.src, u.bytes, nullptr, u.dst, c.stream});
-      at += (u.bytes + 255) & ~std::size_t(255);
+      if (pinned_host(u.src)) {
+        check(cudaMemcpyAsync(u.dst, u.src, u.bytes, cudaMemcpyHostToDevice, c.stream), "copy cells");
+      } else {
+        pageable.push_back(u);
+        total += (u.bytes + 255) & ~std::size_t(255);
+      }
     }
-    check(host_copies(c).run(host), "copy cells");
+    if (!pageable.empty()) {
+      unsigned char* base = c.upload.ensure(total);
+      std::vector<msb::HostCopies::Job> host;
+      std::size_t at = 0;
+      for (const auto& u : pageable) {
+        host.push_back({base + at, u.src, u.bytes, nullptr, u.dst, c.stream});
+        at += (u.bytes + 255) & ~std::size_t(255);
+      }
+      check(host_copies(c).run(host), "copy cells");
+    }
   }
   c.state.ensure(n);
   reset_status(c);

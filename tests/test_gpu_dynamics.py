@@ -244,6 +244,30 @@ def test_device_resident_step_equals_host_step(backend):
     assert np.array_equal(rh.axial_loads, outputs.loads.cpu().numpy())
 
 
+def test_pinned_host_step_equals_pageable_host_step(backend):
+    """A world kept in page-locked host arrays (copied by DMA without the
+    staging buffers) steps to the same bits, with the same outputs, as one
+    in ordinary numpy arrays."""
+    from microsimulator_b200.backend import PinnedCells
+
+    world = workloads.colony_1k(seed=13, n=700, side=38.0, growth_rate=0.5)
+    p = ContactDynamicsParameters(overlap_tolerance=5e-4)
+    pageable = world.copy()
+    rp = backend.advance_contact_dynamics(pageable, None, 0.02, p)
+    cells = PinnedCells(1000)
+    cells.load(world)
+    outputs = cells.outputs()
+    rq = backend.advance_contact_dynamics(cells, None, 0.02, p, outputs=outputs)
+    pinned = world.copy()
+    cells.store(pinned)
+    assert rp.report == rq.report
+    assert np.array_equal(pageable.geometry(), pinned.geometry())
+    assert np.array_equal(rp.center_velocities, outputs[0]) and np.array_equal(rp.axial_loads, outputs[1])
+    assert np.array_equal(rp.length_increments, outputs[2])
+    with pytest.raises(ValueError):
+        backend.advance_contact_dynamics(cells, None, 0.02, p, outputs=(outputs[0][:-1], outputs[1], outputs[2]))
+
+
 def test_steps_are_deterministic(backend):
     """The same step from the same state gives the same bits, on the same
     context and on a fresh one (the reference's thread-invariance test,
