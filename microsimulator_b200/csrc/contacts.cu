@@ -511,6 +511,12 @@ __global__ void narrow_phase_kernel(GeometryView g, const uint2* __restrict__ pa
       if (counts != nullptr) counts[k] = 0;
       continue;
     }
+    if (g.colony_active != nullptr && g.colony_active[g.colony[pair.x]] == 0u) {
+      // A settled colony of a batch takes no part in this round, as in the
+      // broad phase.
+      if (counts != nullptr) counts[k] = 0;
+      continue;
+    }
     if (prm.box_margin >= 0.0f) {
       // Candidates from a wider search (or from another geometry): only
       // the pairs whose boxes at box_margin overlap here are the

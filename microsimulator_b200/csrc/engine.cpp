@@ -1038,7 +1038,7 @@ std::uint32_t find_touches_kept(Ctx& c, Geometry& geometry, const msb_contact_pa
 
 // Whether the last move allows find_touches_kept.
 bool kept_candidates_hold(const Ctx& c) {
-  return c.kept_valid && c.colonies == 0 && std::isfinite(c.displacement) &&
+  return c.kept_valid && std::isfinite(c.displacement) &&
          2.0 * double(c.displacement) <= double(c.kept_margin) - 1.0e-6;
 }
 
@@ -1494,11 +1494,10 @@ Attempt advance_substep(Ctx& c, float dt, const msb_contact_dynamics_parameters&
   }
   mark(c, kPhaseSearch);
   // The first search keeps its candidates, padded by kRecheckReach more than
-  // the candidate margin, for the overlap re-checks of the refinement rounds.
-  const bool keep = c.colonies == 0;
+  // the candidate margin, for the overlap re-checks of the refinement rounds
+  // (in a batch, those of the colonies still searched).
   const std::uint32_t found = find_touches(c, c.state, cp, wp, p.candidate_margin, c.touches,
-                                           keep ? p.candidate_margin + kRecheckReach : p.candidate_margin, keep);
-  if (!keep) c.kept_valid = false;
+                                           p.candidate_margin + kRecheckReach, true);
   mark(c, kPhaseRows);
   c.rows.count = 0;
   c.rows.ensure(std::max<std::uint32_t>(found, 1));
