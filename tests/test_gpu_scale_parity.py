@@ -21,7 +21,7 @@ import numpy as np
 import pytest
 
 from microsimulator_b200 import workloads
-from microsimulator_b200.types import ContactDynamicsParameters, ContactParameters
+from microsimulator_b200.types import ContactDynamicsParameters, ContactParameters, GrowthLoadLaw, GrowthLoadResponse
 
 pytestmark = pytest.mark.gpu
 
@@ -51,10 +51,10 @@ def assert_contacts_equal(backend, reference, world):
         assert actual.tobytes() == expected.tobytes(), margin
 
 
-def tight_step(backend, reference, world, walls):
+def tight_step(backend, reference, world, walls, tight=TIGHT):
     gpu, cpu = world.copy(), world.copy()
-    rg = backend.advance_contact_dynamics(gpu, walls, DT, TIGHT).report
-    rc = reference.advance_contact_dynamics(cpu, walls, DT, TIGHT).report
+    rg = backend.advance_contact_dynamics(gpu, walls, DT, tight).report
+    rc = reference.advance_contact_dynamics(cpu, walls, DT, tight).report
     assert (rg.substeps, rg.halvings) == (rc.substeps, rc.halvings), (rg, rc)
     assert np.array_equal(gpu.ids, cpu.ids)
     spread = float(np.max(np.abs(gpu.geometry()[:, :3] - cpu.geometry()[:, :3])))
@@ -64,7 +64,7 @@ def tight_step(backend, reference, world, walls):
           f"max |direction - reference| {turn:.3e}")
     assert spread <= 1e-4 * RADIUS, spread
     assert turn <= 1e-4, turn
-    assert abs(rg.max_overlap - rc.max_overlap) <= 2 * TIGHT.overlap_tolerance
+    assert abs(rg.max_overlap - rc.max_overlap) <= 2 * tight.overlap_tolerance
 
 
 @pytest.fixture(scope="module")
@@ -96,3 +96,20 @@ def test_trap_colony_tight_step_with_walls_matches_reference(backend, reference)
         actual = backend.find_external_contacts(world, walls, every_face=every_face)
         assert actual.tobytes() == expected.tobytes()
     tight_step(backend, reference, world, walls)
+
+
+@pytest.mark.parametrize("law", [GrowthLoadResponse(GrowthLoadLaw.LINEAR, free_load=0.05, stall_load=0.5),
+                                 GrowthLoadResponse(GrowthLoadLaw.EXPONENTIAL, sensitivity=2.0)])
+def test_load_sensitive_colony_with_fixed_cells_tight_step_matches_reference(backend, reference, law):
+    """200,000 capsules of the jammed distribution whose growth falls with
+    axial load (the growth-load laws of contact_dynamics.cpp:600-612), 5 % of
+    them fixed: one step at tolerance 2e-5 um against the reference's."""
+    world = workloads.jammed(n=200_000, seed=7)
+    world.fixed = (np.random.default_rng(8).random(len(world)) < 0.05).astype(np.uint8)
+    settle_p = ContactDynamicsParameters(overlap_tolerance=5e-4, growth=law)
+    for step in range(3):
+        plan = workloads.plan_divisions(world, 0.02, seed=300 + step)
+        world.divide_many(plan.parents, 0.5, plan.rotations)
+        backend.advance_contact_dynamics(world, None, DT, settle_p)
+        world.next_id = int(world.ids.max()) + 1
+    tight_step(backend, reference, world, None, ContactDynamicsParameters(overlap_tolerance=2e-5, growth=law))
