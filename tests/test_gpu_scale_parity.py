@@ -6,8 +6,9 @@ compiled from its sources (oracle/_ref/libmsref.so).
   bit-exact with the reference's find_cell_contacts_cpu
   (cpp/cpu/cpu_contacts.cpp:168-219), before and after steps that move
   capsules out of the plane and divide 2 % of them.
-* One step of that colony, and of the 100,000-capsule trap colony with its
-  wall boxes, at the tight overlap tolerance of the reference's trajectory
+* One step of that colony, of the 100,000-capsule trap colony with its wall
+  boxes, and of a 200,000-capsule load-sensitive colony with fixed cells, at
+  the tight overlap tolerance of the reference's trajectory
   conformance test (tests/conformance/trajectory_conformance_test.cpp:140-172
   uses 2e-4; 2e-5 here): the same substep structure as the reference's step
   and every position within 1e-4 capsule radius of it.
@@ -98,12 +99,16 @@ def test_trap_colony_tight_step_with_walls_matches_reference(backend, reference)
     tight_step(backend, reference, world, walls)
 
 
-@pytest.mark.parametrize("law", [GrowthLoadResponse(GrowthLoadLaw.LINEAR, free_load=0.05, stall_load=0.5),
-                                 GrowthLoadResponse(GrowthLoadLaw.EXPONENTIAL, sensitivity=2.0)])
-def test_load_sensitive_colony_with_fixed_cells_tight_step_matches_reference(backend, reference, law):
-    """200,000 capsules of the jammed distribution whose growth falls with
-    axial load (the growth-load laws of contact_dynamics.cpp:600-612), 5 % of
-    them fixed: one step at tolerance 2e-5 um against the reference's."""
+def test_load_sensitive_colony_with_fixed_cells_tight_step_matches_reference(backend, reference):
+    """200,000 capsules of the jammed distribution whose growth stalls under
+    axial load (the linear growth-load law of contact_dynamics.cpp:600-612),
+    5 % of them fixed: one step at tolerance 2e-5 um against the
+    reference's.  (The exponential law's exp is FP64 rounded once here and
+    glibc's expf in the reference, one ulp apart at times; in this stiff
+    system, whose solves run into the iteration limit, such a difference can
+    flip a halving decision, so that law is compared in lockstep on small
+    colonies in test_gpu_dynamics.py instead.)"""
+    law = GrowthLoadResponse(GrowthLoadLaw.LINEAR, free_load=0.05, stall_load=0.5)
     world = workloads.jammed(n=200_000, seed=7)
     world.fixed = (np.random.default_rng(8).random(len(world)) < 0.05).astype(np.uint8)
     settle_p = ContactDynamicsParameters(overlap_tolerance=5e-4, growth=law)
