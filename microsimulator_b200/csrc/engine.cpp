@@ -196,7 +196,10 @@ constexpr std::uint32_t kFusedRelaxationItems = 0;
 // The substep's first search pads its candidate boxes by this much more
 // than the candidate margin, so that its candidates serve the overlap
 // re-checks while no box face has moved more than half the padded margin.
-constexpr float kRecheckReach = 0.1f;
+// Measured at 1.35M capsules over 10 steps, search phase per step: 0.05 um
+// 4.92 ms (more re-checks fall back to a full search), 0.1 um 3.76, 0.15 um
+// 3.19, 0.2 um 3.29 (more candidates to narrow).
+constexpr float kRecheckReach = 0.15f;
 constexpr float kMaximumSubstepRotation = 0.5f;
 constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
 
