@@ -26,10 +26,8 @@ __device__ __forceinline__ float growth_factor(std::uint32_t law, float sensitiv
 // drift the additions are of +0.0f, which leaves every value's bits as they
 // are, so the drift arrays are only read when the system has some.
 template <class Desc>
-__device__ __forceinline__ void respond(const Desc& d, std::uint32_t b, const float w[6], float load, float v[6],
-                                        float& rate) {
-  const float4 ba = __ldcs(&d.bodies.a[b]);
-  const float4 bb = __ldcs(&d.bodies.b[b]);
+__device__ __forceinline__ void respond(const Desc& d, std::uint32_t b, float4 ba, float4 bb, const float w[6],
+                                        float load, float v[6], float& rate) {
   float4 da = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   float4 db = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   if (d.has_drift) {
@@ -53,6 +51,12 @@ __device__ __forceinline__ void respond(const Desc& d, std::uint32_t b, const fl
   v[4] += db.y;
   v[5] += db.z;
   rate = bb.z > 0.0f ? bb.z * growth_factor(d.law, d.sensitivity, d.free_load, d.stall_load, load) : bb.z;
+}
+// The same with the body's record read here.
+template <class Desc>
+__device__ __forceinline__ void respond(const Desc& d, std::uint32_t b, const float w[6], float load, float v[6],
+                                        float& rate) {
+  respond(d, b, __ldcs(&d.bodies.a[b]), __ldcs(&d.bodies.b[b]), w, load, v, rate);
 }
 
 // wrench_dot(jacobian, velocity) - lever * rate: one side's term of a row's
