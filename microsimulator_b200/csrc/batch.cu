@@ -328,12 +328,22 @@ int resident_clusters(int cluster) {
 __global__ void colony_row_keys_kernel(const uint2* __restrict__ slots, std::uint32_t rows,
                                        const std::uint32_t* __restrict__ of_slot, std::uint32_t* __restrict__ keys,
                                        std::uint32_t* __restrict__ values, std::uint32_t* __restrict__ counts) {
-  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < rows; i += gridDim.x * blockDim.x) {
-    const std::uint32_t colony = of_slot[slots[i].x];
-    keys[i] = colony;
-    values[i] = i;
-    atomicAdd(&counts[colony], 1u);
+  // Contiguous ranges per warp: rows in first-id order mostly share their
+  // colony with their neighbours, so the counts are folded per warp.
+  const WarpRange range = warp_range(rows);
+  KeyCarry carry;
+  for (std::uint32_t base = range.begin; base < range.end; base += 32) {
+    const std::uint32_t i = base + (threadIdx.x & 31u);
+    const bool live = i < range.end;
+    std::uint32_t colony = 0u;
+    if (live) {
+      colony = of_slot[slots[i].x];
+      keys[i] = colony;
+      values[i] = i;
+    }
+    carry_item<true>(counts, carry, live, colony, 1u);
   }
+  if ((threadIdx.x & 31u) == 0u) carry_flush<true>(counts, carry);
 }
 
 }  // namespace

@@ -82,6 +82,90 @@ __device__ __forceinline__ void raise_status(std::uint32_t* status, std::uint32_
   atomicCAS(status, 0u, code);
 }
 
+// ---- maxima and counts gathered on one address
+//
+// Thousands of warps each issuing an atomic to the same word serialise on
+// it (a jammed colony's millions of overlapping contacts raising one
+// deepest-overlap word).  These helpers fold a thread's, a warp's and a
+// block's values first, so each block issues one atomic per word.
+
+// Non-negative floats order as their bits: a running maximum of the
+// positive values among `value`s, as bits (0: none).
+__device__ __forceinline__ std::uint32_t max_bits(std::uint32_t bits, float value) {
+  return value > 0.0f ? ::max(bits, __float_as_uint(value)) : bits;
+}
+
+// atomicMax(target, bits) of every thread of the block, as one atomic per
+// block.  Every thread of the block calls it (a block barrier).
+__device__ __forceinline__ void block_max_into(std::uint32_t* target, std::uint32_t bits) {
+  __shared__ std::uint32_t block_bits;
+  if (threadIdx.x == 0) block_bits = 0u;
+  __syncthreads();
+  const std::uint32_t w = __reduce_max_sync(0xFFFFFFFFu, bits);
+  if ((threadIdx.x & 31u) == 0u && w != 0u) atomicMax(&block_bits, w);
+  __syncthreads();
+  if (threadIdx.x == 0 && block_bits != 0u) atomicMax(target, block_bits);
+}
+
+// A contiguous range of items per warp (covering [0, count) over the grid),
+// walked 32 at a time by the warp together: items next to each other in
+// memory meet in one warp, so that per-key values of sorted keys can be
+// folded before they are written.
+struct WarpRange {
+  std::uint32_t begin;
+  std::uint32_t end;
+};
+__device__ __forceinline__ WarpRange warp_range(std::uint32_t count) {
+  const std::uint32_t warps = (gridDim.x * blockDim.x) >> 5;
+  const std::uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const std::uint64_t per = ((std::uint64_t(count) + warps - 1) / warps + 31) & ~std::uint64_t(31);
+  const std::uint64_t b = std::uint64_t(warp) * per;
+  return {std::uint32_t(b < count ? b : count), std::uint32_t(b + per < count ? b + per : count)};
+}
+
+// Per-key sums (Sum) or maxima of a warp's items whose keys mostly repeat
+// from one item to the next, as the colonies of rows in first-id order do:
+// lane 0 carries the total of the current key and adds it to targets[key]
+// once the key changes (and at the end, carry_flush); 32 items with more
+// than one key go to their targets lane by lane.  Called by the whole warp
+// with lane 0 live.
+struct KeyCarry {
+  std::uint32_t key = 0xFFFFFFFFu;
+  std::uint32_t value = 0u;
+};
+template <bool Sum>
+__device__ __forceinline__ void carry_flush(std::uint32_t* targets, const KeyCarry& carry) {
+  if (carry.key != 0xFFFFFFFFu && carry.value != 0u) {
+    if constexpr (Sum) {
+      atomicAdd(targets + carry.key, carry.value);
+    } else {
+      atomicMax(targets + carry.key, carry.value);
+    }
+  }
+}
+template <bool Sum>
+__device__ __forceinline__ void carry_item(std::uint32_t* targets, KeyCarry& carry, bool live, std::uint32_t key,
+                                           std::uint32_t value) {
+  const std::uint32_t key0 = __shfl_sync(0xFFFFFFFFu, key, 0);
+  if (__all_sync(0xFFFFFFFFu, !live || key == key0)) {
+    const std::uint32_t v = live ? value : 0u;
+    const std::uint32_t w = Sum ? __reduce_add_sync(0xFFFFFFFFu, v) : __reduce_max_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31u) == 0u) {
+      if (carry.key != key0) {
+        carry_flush<Sum>(targets, carry);
+        carry = {key0, 0u};
+      }
+      carry.value = Sum ? carry.value + w : ::max(carry.value, w);
+    }
+  } else if (live && value != 0u) {
+    if constexpr (Sum) {
+      atomicAdd(targets + key, value);
+    } else {
+      atomicMax(targets + key, value);
+    }
+  }
+}
+
 // Index checks of the checked build (MSB_DEVICE_CHECKS=1, libmsb200_checked.so):
 // an index at or past its bound records kStatusIndex in *status and the
 // caller skips the access.  In the ordinary build the check is compiled out.

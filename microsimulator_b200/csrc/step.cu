@@ -104,50 +104,64 @@ __global__ void make_rows_kernel(const Touch* __restrict__ touches, std::uint32_
                                  RowBuild prm, ResponseArrays response, int correct, RowArrays rows,
                                  std::uint32_t row_base, std::uint64_t* __restrict__ key_partner,
                                  float* __restrict__ multipliers, std::uint32_t* overlap_bits, Colonies colonies) {
-  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-    const Touch t = touches[k];
-    const bool wall = t.s2 == kInvalidSlot;
-    const std::uint32_t colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
-    const float stiffness = colonies.of_slot != nullptr ? colonies.stiffness[colony] : prm.contact_stiffness;
-    const float compliance = 1.0f / (wall ? prm.wall_stiffness : stiffness);
-    float offset = smax(t.sep, -prm.recovery);
-    const float c = t.sep < -prm.recovery ? compliance * prm.recovery / -t.sep : compliance;
-    const F3 n{t.normal[0], t.normal[1], t.normal[2]};
-    const F3 p{t.point[0], t.point[1], t.point[2]};
-    const float4 pl1 = geometry.pos_len[t.s1];
-    const float4 dr1 = geometry.dir_rad[t.s1];
-    const F3 a1 = cross(p - xyz(pl1), n);
-    const float l1 = length_lever(pl1, dr1, p - n * dr1.w, n);
-    float4 ra = make_float4(-n.x, -n.y, -n.z, -a1.x);
-    float4 rb = make_float4(-a1.y, -a1.z, l1, offset);
-    float4 rc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    float4 rd = make_float4(0.0f, 0.0f, 0.0f, c);
-    if (!wall) {
-      const float4 pl2 = geometry.pos_len[t.s2];
-      const float4 dr2 = geometry.dir_rad[t.s2];
-      const F3 a2 = cross(p - xyz(pl2), n);
-      const float l2 = length_lever(pl2, dr2, p + n * (t.sep + dr2.w), n * -1.0f);
-      rc = make_float4(n.x, n.y, n.z, a2.x);
-      rd = make_float4(a2.y, a2.z, l2, c);
+  // Each warp takes a contiguous range of contacts, so that the deepest
+  // overlap of each colony is folded per warp before it is written.
+  const WarpRange range = warp_range(count);
+  std::uint32_t deepest = 0u;
+  KeyCarry carry;
+  for (std::uint32_t base = range.begin; base < range.end; base += 32) {
+    const std::uint32_t k = base + (threadIdx.x & 31u);
+    const bool live = k < range.end;
+    std::uint32_t colony = 0u;
+    std::uint32_t depth = 0u;
+    if (live) {
+      const Touch t = touches[k];
+      const bool wall = t.s2 == kInvalidSlot;
+      colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
+      const float stiffness = colonies.of_slot != nullptr ? colonies.stiffness[colony] : prm.contact_stiffness;
+      const float compliance = 1.0f / (wall ? prm.wall_stiffness : stiffness);
+      float offset = smax(t.sep, -prm.recovery);
+      const float c = t.sep < -prm.recovery ? compliance * prm.recovery / -t.sep : compliance;
+      const F3 n{t.normal[0], t.normal[1], t.normal[2]};
+      const F3 p{t.point[0], t.point[1], t.point[2]};
+      const float4 pl1 = geometry.pos_len[t.s1];
+      const float4 dr1 = geometry.dir_rad[t.s1];
+      const F3 a1 = cross(p - xyz(pl1), n);
+      const float l1 = length_lever(pl1, dr1, p - n * dr1.w, n);
+      float4 ra = make_float4(-n.x, -n.y, -n.z, -a1.x);
+      float4 rb = make_float4(-a1.y, -a1.z, l1, offset);
+      float4 rc = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      float4 rd = make_float4(0.0f, 0.0f, 0.0f, c);
+      if (!wall) {
+        const float4 pl2 = geometry.pos_len[t.s2];
+        const float4 dr2 = geometry.dir_rad[t.s2];
+        const F3 a2 = cross(p - xyz(pl2), n);
+        const float l2 = length_lever(pl2, dr2, p + n * (t.sep + dr2.w), n * -1.0f);
+        rc = make_float4(n.x, n.y, n.z, a2.x);
+        rd = make_float4(a2.y, a2.z, l2, c);
+      }
+      if (correct) {
+        // predicted_rate (contact_dynamics.cpp:286-301)
+        float rate = wrench_dot(ra, rb, response.a[t.s1], response.b[t.s1]) - rb.z * response.a[t.s1].w;
+        if (!wall) rate += wrench_dot(rc, rd, response.a[t.s2], response.b[t.s2]) - rd.z * response.a[t.s2].w;
+        offset -= prm.dt * rate;
+        rb.w = offset;
+      }
+      const std::uint32_t i = row_base + k;
+      rows.a[i] = ra;
+      rows.b[i] = rb;
+      rows.c[i] = rc;
+      rows.d[i] = rd;
+      rows.slots[i] = make_uint2(t.s1, t.s2);
+      key_partner[i] = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
+      multipliers[i] = 0.0f;
+      depth = max_bits(0u, -t.sep);
+      deepest = ::max(deepest, depth);
     }
-    if (correct) {
-      // predicted_rate (contact_dynamics.cpp:286-301)
-      float rate = wrench_dot(ra, rb, response.a[t.s1], response.b[t.s1]) - rb.z * response.a[t.s1].w;
-      if (!wall) rate += wrench_dot(rc, rd, response.a[t.s2], response.b[t.s2]) - rd.z * response.a[t.s2].w;
-      offset -= prm.dt * rate;
-      rb.w = offset;
-    }
-    const std::uint32_t i = row_base + k;
-    rows.a[i] = ra;
-    rows.b[i] = rb;
-    rows.c[i] = rc;
-    rows.d[i] = rd;
-    rows.slots[i] = make_uint2(t.s1, t.s2);
-    key_partner[i] = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
-    multipliers[i] = 0.0f;
-    atomic_max_nonnegative(overlap_bits, -t.sep);
-    if (colonies.overlap_bits != nullptr) atomic_max_nonnegative(colonies.overlap_bits + colony, -t.sep);
+    if (colonies.overlap_bits != nullptr) carry_item<false>(colonies.overlap_bits, carry, live, colony, depth);
   }
+  if (colonies.overlap_bits != nullptr && (threadIdx.x & 31u) == 0u) carry_flush<false>(colonies.overlap_bits, carry);
+  block_max_into(overlap_bits, deepest);
 }
 
 // ForceMemory::force with the occurrence rule of advance_substep
@@ -213,6 +227,7 @@ __device__ __forceinline__ bool rotate_axis_angle(F3 d, F3 rot, float max_rot, F
 __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArrays response, float dt,
                             GeometryBuffers trial, std::uint32_t* rotation_bits, std::uint32_t* invalid,
                             std::uint32_t* status, std::uint32_t* displacement_bits) {
+  std::uint32_t largest_rotation = 0u, largest_move = 0u;
   for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const float4 va = response.a[s];
     const float4 vb = response.b[s];
@@ -222,7 +237,7 @@ __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArray
       continue;
     }
     const float angle = norm(rot);
-    atomic_max_nonnegative(rotation_bits, angle);
+    largest_rotation = max_bits(largest_rotation, angle);
     if (angle > kMaximumSubstepRotation) {
       atomicExch(invalid, 1u);
       continue;
@@ -252,9 +267,11 @@ __global__ void move_kernel(std::uint32_t n, GeometryBuffers base, ResponseArray
 #pragma unroll
       for (int k = 0; k < 6; ++k) moved = fmax(moved, fabs(to[k] - from[k]));
       const float bound = isfinite(moved) ? __double2float_ru(moved) : __int_as_float(0x7F800000);
-      atomic_max_nonnegative(displacement_bits, bound);
+      largest_move = max_bits(largest_move, bound);
     }
   }
+  block_max_into(rotation_bits, largest_rotation);
+  if (displacement_bits != nullptr) block_max_into(displacement_bits, largest_move);
 }
 
 __global__ void guess_response_kernel(std::uint32_t n, const float4* __restrict__ guess, BodyArrays bodies,
@@ -329,11 +346,13 @@ __global__ void guess_forces_row_kernel(std::uint32_t rows, const float* __restr
 
 __global__ void largest_rotation_kernel(std::uint32_t n, ResponseArrays response, float dt,
                                         std::uint32_t* rotation_bits) {
+  std::uint32_t largest = 0u;
   for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < n; s += gridDim.x * blockDim.x) {
     const float4 vb = response.b[s];
     const float angle = norm(F3{vb.x * dt, vb.y * dt, vb.z * dt});
-    atomic_max_nonnegative(rotation_bits, isfinite(angle) ? angle : __int_as_float(0x7F800000));
+    largest = max_bits(largest, isfinite(angle) ? angle : __int_as_float(0x7F800000));
   }
+  block_max_into(rotation_bits, largest);
 }
 
 __global__ void restore_kernel(std::uint32_t n, GeometryBuffers src, GeometryBuffers dst, std::uint32_t* status) {
@@ -353,25 +372,44 @@ __global__ void restore_kernel(std::uint32_t n, GeometryBuffers src, GeometryBuf
 __global__ void recheck_kernel(const Touch* __restrict__ touches, std::uint32_t count, KeyedLists current,
                                const float* slack_ptr, float wall_stiffness, float contact_stiffness,
                                std::uint32_t* __restrict__ flags, std::uint32_t* overlap_bits, Colonies colonies) {
-  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < count; k += gridDim.x * blockDim.x) {
-    const Touch t = touches[k];
-    atomic_max_nonnegative(overlap_bits, -t.sep);
-    const std::uint32_t colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
-    if (colonies.overlap_bits != nullptr) atomic_max_nonnegative(colonies.overlap_bits + colony, -t.sep);
-    const float slack = colonies.slack != nullptr ? colonies.slack[colony] : *slack_ptr;
-    if (colonies.stiffness != nullptr) contact_stiffness = colonies.stiffness[colony];
-    const bool wall = t.s2 == kInvalidSlot;
-    const std::uint64_t key = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
-    float force = 0.0f;
-    for (std::uint32_t j = current.offsets[t.s1]; j < current.offsets[t.s1 + 1]; ++j) {
-      const std::uint32_t r = current.rows[j];
-      if (current.partner[r] == key) force += current.multipliers[r];
+  // Contiguous ranges per warp, as in make_rows_kernel: the per-colony
+  // deepest overlaps and flag counts are folded per warp.
+  const WarpRange range = warp_range(count);
+  std::uint32_t deepest = 0u;
+  KeyCarry deepest_carry, flagged_carry;
+  for (std::uint32_t base = range.begin; base < range.end; base += 32) {
+    const std::uint32_t k = base + (threadIdx.x & 31u);
+    const bool live = k < range.end;
+    std::uint32_t colony = 0u;
+    std::uint32_t depth = 0u;
+    std::uint32_t flagged = 0u;
+    if (live) {
+      const Touch t = touches[k];
+      depth = max_bits(0u, -t.sep);
+      deepest = ::max(deepest, depth);
+      colony = colonies.of_slot != nullptr ? colonies.of_slot[t.s1] : 0u;
+      const float slack = colonies.slack != nullptr ? colonies.slack[colony] : *slack_ptr;
+      if (colonies.stiffness != nullptr) contact_stiffness = colonies.stiffness[colony];
+      const bool wall = t.s2 == kInvalidSlot;
+      const std::uint64_t key = wall ? (kWallTag | t.partner) : std::uint64_t(t.s2);
+      float force = 0.0f;
+      for (std::uint32_t j = current.offsets[t.s1]; j < current.offsets[t.s1 + 1]; ++j) {
+        const std::uint32_t r = current.rows[j];
+        if (current.partner[r] == key) force += current.multipliers[r];
+      }
+      const float compliance = 1.0f / (wall ? wall_stiffness : contact_stiffness);
+      const float allowed = slack + force * compliance;
+      flagged = t.sep < -allowed ? 1u : 0u;
+      flags[k] = flagged;
     }
-    const float compliance = 1.0f / (wall ? wall_stiffness : contact_stiffness);
-    const float allowed = slack + force * compliance;
-    flags[k] = t.sep < -allowed ? 1u : 0u;
-    if (flags[k] != 0u && colonies.flagged != nullptr) atomicAdd(colonies.flagged + colony, 1u);
+    if (colonies.overlap_bits != nullptr) carry_item<false>(colonies.overlap_bits, deepest_carry, live, colony, depth);
+    if (colonies.flagged != nullptr) carry_item<true>(colonies.flagged, flagged_carry, live, colony, flagged);
   }
+  if ((threadIdx.x & 31u) == 0u) {
+    if (colonies.overlap_bits != nullptr) carry_flush<false>(colonies.overlap_bits, deepest_carry);
+    if (colonies.flagged != nullptr) carry_flush<true>(colonies.flagged, flagged_carry);
+  }
+  block_max_into(overlap_bits, deepest);
 }
 
 __global__ void gather_flagged_kernel(const Touch* __restrict__ touches, std::uint32_t count,
