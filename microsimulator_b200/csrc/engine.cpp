@@ -1172,7 +1172,7 @@ SolveOutcome solve(Ctx& c, float dt, const msb_growth_load_response& growth, flo
     launch_evaluate(c.desc, std::max(1, grid_for(c.n, kSolveThreads)), false, c.stream);
     return {};
   }
-  c.partials.ensure(5ull * 1184);
+  c.partials.ensure(5ull * kMaxPassBlocks);
   const bool fused = use_fused_relaxation(c, std::max(rows, c.n));
   if (fused) {
     // One cooperative launch runs the whole solve (relax_kernel).
@@ -2445,7 +2445,7 @@ int msb_contact_system_diagonal_bound(msb_context* context, const msb_contact_sy
     c.resp_a.ensure(std::max<std::uint32_t>(c.n, 1));
     c.resp_b.ensure(std::max<std::uint32_t>(c.n, 1));
     auto& graph = graph_for(c, std::max(c.rows.count, c.n));
-    c.partials.ensure(5ull * 1184);
+    c.partials.ensure(5ull * kMaxPassBlocks);
     fill_desc(c, c.rows.count, system->dt, system->growth, 1.0f, 0);
     check(cudaError_t(graph.launch(c.stream)), "launch");
     check(cudaMemcpyAsync(c.host_desc, c.desc, sizeof(SolveDesc), cudaMemcpyDeviceToHost, c.stream), "read");

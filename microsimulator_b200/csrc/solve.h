@@ -162,5 +162,7 @@ void launch_unpack_iterate(SolveDesc* desc, int blocks, cudaStream_t stream);
 void launch_iteration(SolveDesc* desc, int blocks, cudaEvent_t between, cudaStream_t stream);
 
 constexpr int kSolveThreads = 256;
+// Blocks of a BB pass at most: the per-block partials hold this many.
+constexpr int kMaxPassBlocks = 1184;
 
 }  // namespace msb
