@@ -229,3 +229,32 @@ def test_batch_with_empty_and_single_cell_colonies(backend):
     # The overlapping pair pushed apart symmetrically.
     px = batch.worlds[4].position_x
     assert px[0] < -1.4 and px[1] > 1.4 and abs(float(px[0] + px[1])) < 1e-4
+
+
+def test_colonies_with_interleaved_ids_step_as_with_grouped_ids():
+    """Rows in first-id order are grouped by colony when each colony's ids
+    are a block (as the sweep tags them), and interleaved when the colonies'
+    ids alternate.  The per-colony deepest overlaps, flag counts and row
+    counts are folded per warp where a warp's rows share a colony and added
+    lane by lane where they do not; either way each colony's step is the
+    same: with the same order of ids within every colony, the same bits."""
+    worlds = settled_worlds()
+    grouped = sweep.concatenate(worlds)
+    interleaved = grouped.copy()
+    colony = np.repeat(np.arange(len(worlds), dtype=np.uint64), [len(w) for w in worlds])
+    local = np.concatenate([w.ids for w in worlds]).astype(np.uint64)
+    interleaved.ids = local * np.uint64(len(worlds)) + colony
+    interleaved.next_id = int(interleaved.ids.max()) + 1
+    counts = np.array([len(w) for w in worlds], dtype=np.uint32)
+    dyn = ContactDynamicsParameters(overlap_tolerance=TOLERANCE)
+    b = B200Backend(0)
+    try:
+        ra, ca = b.advance_contact_dynamics_batch(grouped, counts, DRAG, STIFFNESS, DT, dyn)
+        rb, cb = b.advance_contact_dynamics_batch(interleaved, counts, DRAG, STIFFNESS, DT, dyn)
+    finally:
+        b.close()
+    assert (ra.substeps, ra.refinements) == (rb.substeps, rb.refinements)
+    assert np.array_equal(ca["rows"], cb["rows"])
+    assert np.array_equal(ca["iterations"], cb["iterations"])
+    assert np.array_equal(ca["max_overlap"], cb["max_overlap"])
+    assert np.array_equal(grouped.geometry(), interleaved.geometry())
