@@ -517,11 +517,13 @@ def sweep_arm(args, backend, local, rank, dist):
     before = [w.copy() for w in batch.worlds]
     total_ms, cell_steps, iterations = 0.0, 0, 0
     phases = {name: 0.0 for name in backend.PHASES}
+    steps_ms = []
     if dist is not None:
         dist.barrier()
     for k in range(args.steps):
         ms, report, colonies, n = step(100 + k)
         total_ms += ms
+        steps_ms.append(round(ms, 2))
         cell_steps += n
         iterations += int(colonies["iterations"].sum())
         converged = int((colonies["status"] == 0).sum())
@@ -560,6 +562,7 @@ def sweep_arm(args, backend, local, rank, dist):
         "ms_per_step": total_ms / args.steps,
         "bb_iterations_per_step_summed_over_colonies": iterations / args.steps,
         "phase_ms_per_step": phases,
+        "steps_ms": steps_ms,
         "colonies_converged_last_step": f"{converged} of {len(batch)} on this rank",
         "deepest_overlap_last_step_um": deepest,
         "tuning": tuning,
@@ -575,7 +578,7 @@ def compact(arm):
         return None
     out = {}
     for key, value in arm.items():
-        if key in ("workload", "phase_ms_per_step", "sharding", "sample", "how", "timing"):
+        if key in ("workload", "phase_ms_per_step", "sharding", "sample", "how", "timing", "steps_ms"):
             continue
         out[key] = compact(value) if isinstance(value, dict) else value
     return out
