@@ -17,12 +17,14 @@ namespace msb {
 namespace {
 
 // Response of the colony's bodies to its (projected, with project)
-// multipliers; each thread keeps kBatch entries' gathers in flight.
+// multipliers; each thread keeps kBatch entries' gathers in flight.  Inside
+// the iterations each row's multiplier and gap come as one float2 (the
+// iterate), one gather instead of two: the 256-colony sweep's solve phase
+// measured 40.6-41.1 -> 39.1 ms per step, the same iterations and bits.
 template <int kBatch>
 __device__ void colony_body_pass(const BatchDesc& d, std::uint32_t b0, std::uint32_t b1, std::uint32_t tid,
                                  std::uint32_t stride, bool project, float alpha) {
   const float* g = d.multipliers;
-  const float* gap = d.gaps;
   for (std::uint32_t b = b0 + tid; b < b1; b += stride) {
     float w[6] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
     float load = 0.0f;
@@ -42,8 +44,14 @@ __device__ void colony_body_pass(const BatchDesc& d, std::uint32_t b0, std::uint
       for (int t = 0; t < kBatch; ++t) {
         if (k0 + t < end) {
           const std::uint32_t row = __float_as_uint(eb[t].w) >> 1;  // side bits: row << 1 | side
-          gv[t] = __ldcg(&g[row]);
-          pv[t] = project ? __ldcg(&gap[row]) : 0.0f;
+          if (project) {
+            const float2 q = __ldcg(&d.iterate[row]);  // (multiplier, gap) in one gather
+            gv[t] = q.x;
+            pv[t] = q.y;
+          } else {
+            gv[t] = __ldcg(&g[row]);
+            pv[t] = 0.0f;
+          }
         }
       }
 #pragma unroll
@@ -76,15 +84,22 @@ struct Sums {
 };
 
 // Gaps of the colony's rows (and, with project, one projected step with its
-// BB products).
+// BB products), written with the rows' multipliers into the iterate; the
+// initial pass reads the multipliers array, the projected ones the iterate.
 __device__ Sums colony_row_pass(const BatchDesc& d, std::uint32_t r0, std::uint32_t r1, std::uint32_t tid,
                                 std::uint32_t stride, bool project, float alpha) {
   Sums s{0.0, 0.0, 0.0, 0.0f, true};
   const float dt = d.dt;
   for (std::uint32_t j = r0 + tid; j < r1; j += stride) {
     const std::uint32_t i = d.colony_rows[j];
-    const float gi = __ldcg(&d.multipliers[i]);
-    const float gpi = project ? __ldcg(&d.gaps[i]) : 0.0f;
+    float gi, gpi = 0.0f;
+    if (project) {
+      const float2 q = __ldcg(&d.iterate[i]);
+      gi = q.x;
+      gpi = q.y;
+    } else {
+      gi = __ldcg(&d.multipliers[i]);
+    }
     const uint2 sl = __ldcs(&d.rows.slots[i]);
     const float4 ra = __ldcs(&d.rows.a[i]);
     const float4 rb = __ldcs(&d.rows.b[i]);
@@ -110,9 +125,8 @@ __device__ Sums colony_row_pass(const BatchDesc& d, std::uint32_t r0, std::uint3
       s.ss += moved * moved;
       s.sy += moved * change;
       s.yy += change * change;
-      __stcg(&d.multipliers[i], m);
     }
-    __stcg(&d.gaps[i], gn);
+    __stcg(&d.iterate[i], make_float2(m, gn));
   }
   return s;
 }
@@ -269,6 +283,14 @@ __global__ void __launch_bounds__(Threads, Lean ? 1024 / Threads : 1) batch_solv
         proceed_s = proceed;
       }
       __syncthreads();
+    }
+    // Each thread's rows of the last row pass back into the multiplier and
+    // gap arrays.
+    for (std::uint32_t j = r0 + tid; j < r1; j += stride) {
+      const std::uint32_t i = d.colony_rows[j];
+      const float2 q = __ldcg(&d.iterate[i]);
+      d.multipliers[i] = q.x;
+      d.gaps[i] = q.y;
     }
     if (rank == 0 && threadIdx.x == 0) d.state[colony] = {step, residual, colony_bound, iterations, status};
     // The next claim's two barriers order every remote read of this colony's

@@ -29,6 +29,7 @@ struct BatchDesc {
   ResponseArrays response;
   float* multipliers;
   float* gaps;
+  float2* iterate;  // (multiplier, gap) of each row inside a solve
   const std::uint32_t* colony_rows;   // row indices grouped by colony, row order within one
   const std::uint32_t* row_offsets;   // colonies + 1
   const std::uint32_t* cell_offsets;  // colonies + 1: a colony's bodies are a slot range

@@ -1214,6 +1214,7 @@ msb::BatchDesc batch_desc(Ctx& c, float dt, const msb_growth_load_response& grow
   d.response = {c.resp_a.p, c.resp_b.p};
   d.multipliers = c.rows.multipliers.p;
   d.gaps = c.rows.gaps.p;
+  d.iterate = c.rows.iterate.p;
   d.colony_rows = c.colony_rows.p;
   d.row_offsets = c.colony_row_offsets.p;
   d.cell_offsets = c.colony_offsets.p;
