@@ -506,6 +506,9 @@ __global__ void narrow_phase_kernel(GeometryView g, const uint2* __restrict__ pa
                                     std::uint32_t* status) {
   for (std::uint64_t k = blockIdx.x * std::uint64_t(blockDim.x) + threadIdx.x; k < pair_count;
        k += std::uint64_t(gridDim.x) * blockDim.x) {
+    // The fill pass skips the pairs that the count pass found without a
+    // touch (most of a padded candidate list): no geometry loads for them.
+    if (touches != nullptr && offsets[k + 1] == offsets[k]) continue;
     const uint2 pair = pairs[k];
     if (!index_ok(pair.x, g.count, status) || !index_ok(pair.y, g.count, status)) {
       if (counts != nullptr) counts[k] = 0;

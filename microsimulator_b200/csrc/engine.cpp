@@ -909,8 +909,12 @@ std::uint32_t narrow_touches(Ctx& c, const GeometryView& g, ContactSearchParams 
   check(cudaMemsetAsync(c.pair_counts.p + pair_count, 0, 4, c.stream), "memset");
   launch_narrow_phase(g, pairs, pair_count, prm, c.pair_counts.p, nullptr, nullptr, c.stream, c.scalars.p + kStatus);
   exclusive_scan(c.pair_counts.p, c.pair_offsets.p, pair_count + 1ull, c.temp.p, c.stream);
-  const std::uint32_t touch_count = read_u32(c, c.pair_offsets.p + pair_count);
+  // The touch total and the status words in one round trip.
+  check(cudaMemcpyAsync(c.host_scalars + kScalarCount + 5, c.pair_offsets.p + pair_count, 4, cudaMemcpyDeviceToHost,
+                        c.stream),
+        "read");
   read_scalars(c);
+  const std::uint32_t touch_count = c.host_scalars[kScalarCount + 5];
   if (touch_count == 0) return 0;
   out.ensure(touch_count + 1ull);
   launch_narrow_phase(g, pairs, pair_count, prm, nullptr, c.pair_offsets.p, out.p, c.stream, c.scalars.p + kStatus);
