@@ -434,6 +434,20 @@ typedef struct msb_solve_record {
 int msb_last_step_solves(const msb_context* context, msb_solve_record* records, uint32_t capacity,
                          uint32_t* count);
 
+/* The overlap re-checks of the last msb_advance_contact_dynamics(_device)
+ * or batch call by how their pair candidates were found: a full contact
+ * search, the substep's kept candidates (no cell moved further than their
+ * padding allows), or the kept candidates of the cells that did not merged
+ * with a search of the cells that did (a partial re-search).  Every kind
+ * gives the touches of a full search in its order.  A diagnostic with no
+ * counterpart in the reference. */
+int msb_last_step_searches(const msb_context* context, uint32_t* full, uint32_t* kept, uint32_t* partial);
+
+/* Which re-check kinds the stepper may use (a diagnostic with no
+ * counterpart in the reference): 0 all (the default), 1 no partial
+ * re-search, 2 a full search for every re-check. */
+int msb_set_search_reuse(msb_context* context, uint32_t mode);
+
 /* The form of the BB relaxation on the device (no counterpart in the
  * reference, whose CUDA backend synchronises with the host every iteration,
  * cpp/cuda/cuda_backend.cu:1397-1400):

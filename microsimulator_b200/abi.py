@@ -436,6 +436,8 @@ SIGNATURES = {
     "msb_set_warm_start_network": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
     "msb_set_motion_guess": (c_int, [c_void_p, c_void_p, c_uint64, c_float]),
     "msb_last_step_solves": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p]),
+    "msb_last_step_searches": (c_int, [c_void_p, c_void_p, c_void_p, c_void_p]),
+    "msb_set_search_reuse": (c_int, [c_void_p, c_uint32]),
     "msb_solve_contact_forces_no_alloc": (
         c_int,
         [

@@ -172,6 +172,20 @@ class B200Backend:
         self._check(status)
         return out[: count.value].copy()
 
+    def last_step_searches(self) -> dict:
+        """The last step's overlap re-checks by how their candidates were
+        found: a full search, the substep's kept candidates, or the kept
+        candidates with a partial re-search of the cells that moved."""
+        full, kept, partial = c_uint32(0), c_uint32(0), c_uint32(0)
+        self._check(self._lib.msb_last_step_searches(self._handle, ctypes.byref(full), ctypes.byref(kept),
+                                                     ctypes.byref(partial)))
+        return {"full": full.value, "kept": kept.value, "partial": partial.value}
+
+    def set_search_reuse(self, mode: int) -> None:
+        """0: the re-checks use every kind of search (the default); 1: no
+        partial re-search; 2: a full search each time."""
+        self._check(self._lib.msb_set_search_reuse(self._handle, mode))
+
     PHASES = ("load", "search", "rows", "incidence", "solve", "move", "output", "guess")
 
     def last_step_phases(self) -> dict:

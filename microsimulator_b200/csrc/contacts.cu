@@ -382,6 +382,174 @@ __global__ void compact_slab_kernel(std::uint32_t n, const std::uint32_t* __rest
   }
 }
 
+// ---------------------------------------------------------- partial re-search
+//
+// An overlap re-check whose substep's kept candidates (padded by a margin P
+// at the substep's base geometry) may no longer cover every pair, because
+// some cells moved more than P / 2 since: the pairs of two cells that each
+// moved less are still covered, and the pairs of the others ("fast" cells)
+// are searched again on a grid of the current geometry.  Those not already
+// kept (usually none: the kept list's padding covers most of a fast cell's
+// move) are merged into the kept list in (first id, second id) order.
+
+// Cells whose unpadded box moved by more than the kept candidates allow
+// between `from` and `to` (a face moved by `bound`, rounded up as the move
+// kernel rounds it, with 2 * bound > allowance), appended to `list` in any
+// order; *count their number.  Cells of a batch's settled colonies are left
+// out, as their pairs are in every search of the round.
+__global__ void fast_cells_kernel(GeometryView from, GeometryView to, double allowance, std::uint32_t* __restrict__ fast,
+                                  std::uint32_t* __restrict__ list, std::uint32_t* count) {
+  for (std::uint32_t s = blockIdx.x * blockDim.x + threadIdx.x; s < to.count; s += gridDim.x * blockDim.x) {
+    double a[6], b[6];
+    padded_box(from.pos_len[s], from.dir_rad[s], 0.0f, a);
+    padded_box(to.pos_len[s], to.dir_rad[s], 0.0f, b);
+    double moved = 0.0;
+#pragma unroll
+    for (int k = 0; k < 6; ++k) moved = fmax(moved, fabs(b[k] - a[k]));
+    const float bound = isfinite(moved) ? __double2float_ru(moved) : __int_as_float(0x7F800000);
+    bool f = !(2.0 * double(bound) <= allowance);
+    if (f && to.colony_active != nullptr && to.colony_active[to.colony[s]] == 0u) f = false;
+    fast[s] = f ? 1u : 0u;
+    if (f) list[atomicAdd(count, 1u)] = s;
+  }
+}
+
+// (ids[first], ids[second]) of pair p is below that of pair q.
+__device__ __forceinline__ bool pair_before(const std::uint64_t* ids, uint2 p, uint2 q) {
+  const std::uint64_t a = ids[p.x], b = ids[q.x];
+  return a < b || (a == b && ids[p.y] < ids[q.y]);
+}
+
+// The first of `count` pairs sorted by (first id, second id) that is not
+// before pair p.
+__device__ __forceinline__ std::uint32_t lower_bound_pair(const uint2* sorted, std::uint32_t count,
+                                                          const std::uint64_t* ids, uint2 p) {
+  std::uint32_t lo = 0, hi = count;
+  while (lo < hi) {
+    const std::uint32_t mid = lo + (hi - lo) / 2;
+    if (pair_before(ids, sorted[mid], p)) {
+      lo = mid + 1;
+    } else {
+      hi = mid;
+    }
+  }
+  return lo;
+}
+
+// The partners of each listed fast cell on the grid of the current
+// geometry (boxes at margin 0): every cell whose FP64 box overlaps its own,
+// except another fast cell of lower id (whose own query lists that pair) and
+// the pairs the kept list holds.  Count pass (pairs null): counts[i]; fill
+// pass: the pairs at offsets[i], each as (lower-id slot, higher-id slot).
+// The listed cells' number is read from *fast_count.
+__global__ void fast_partners_kernel(GeometryView g, const double* __restrict__ bounds, const GridParams* grid_ptr,
+                                     const std::uint32_t* __restrict__ starts, const float4* __restrict__ sorted_lo,
+                                     const float4* __restrict__ sorted_hi, const std::uint64_t* __restrict__ sorted_id,
+                                     const std::int64_t* __restrict__ coords, const std::uint32_t* __restrict__ fast,
+                                     const std::uint32_t* __restrict__ list, const std::uint32_t* fast_count_ptr,
+                                     std::uint32_t cap, const uint2* __restrict__ kept, std::uint32_t kept_count,
+                                     std::uint32_t* __restrict__ counts, const std::uint32_t* __restrict__ offsets,
+                                     uint2* __restrict__ pairs) {
+  const GridParams grid = *grid_ptr;
+  const std::uint32_t fast_count = *fast_count_ptr < cap ? *fast_count_ptr : cap;
+  for (std::uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cap; i += gridDim.x * blockDim.x) {
+    if (grid.status != 0 || i >= fast_count) {
+      if (pairs == nullptr) counts[i] = 0;
+      continue;
+    }
+    const std::uint32_t f = list[i];
+    const std::uint32_t colony = g.colony != nullptr ? g.colony[f] : 0u;
+    double box[6];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) box[q] = bounds[6 * std::uint64_t(f) + q];
+    const float4 my_lo = make_float4(__double2float_rd(box[0]), __double2float_rd(box[1]), __double2float_rd(box[2]), 0.0f);
+    const float4 my_hi = make_float4(__double2float_ru(box[3]), __double2float_ru(box[4]), __double2float_ru(box[5]), 0.0f);
+    const std::uint64_t id = g.ids[f];
+    std::int64_t at[3];
+    box_of(box, grid, at, colony);
+    std::int64_t first[3], last[3];
+#pragma unroll
+    for (int q = 0; q < 3; ++q) {
+      first[q] = at[q] == 0 ? 0 : at[q] - 1;
+      last[q] = smin(std::int64_t(grid.dims[q]) - 1, at[q] + 1);
+    }
+    if (grid.colony_stride > 0) {
+      const std::int64_t own = std::int64_t(colony) * std::int64_t(grid.colony_stride);
+      first[2] = smax(first[2], own);
+      last[2] = smin(last[2], own + std::int64_t(grid.colony_stride) - 3);
+    }
+    const std::uint32_t base = pairs != nullptr ? offsets[i] : 0u;
+    std::uint32_t found = 0;
+    for (std::int64_t x = first[0]; x <= last[0]; ++x) {
+      for (std::int64_t y = first[1]; y <= last[1]; ++y) {
+        for (std::int64_t z = first[2]; z <= last[2]; ++z) {
+          const std::uint32_t b = bucket_of(grid, x, y, z);
+          const std::uint32_t end = starts[b + 1];
+          for (std::uint32_t m = starts[b]; m < end; ++m) {
+            const float4 lo = sorted_lo[m];
+            const std::uint32_t j = __float_as_uint(lo.w);
+            if (j == f) continue;
+            const std::uint64_t other = sorted_id[m];
+            if (fast[j] != 0u && other < id) continue;
+            const float4 hi = sorted_hi[m];
+            if (!(my_hi.x >= lo.x && hi.x >= my_lo.x && my_hi.y >= lo.y && hi.y >= my_lo.y && my_hi.z >= lo.z &&
+                  hi.z >= my_lo.z)) {
+              continue;
+            }
+            if (grid.hashed) {
+              const std::int64_t* c = coords + 3 * std::uint64_t(j);
+              if (c[0] != x || c[1] != y || c[2] != z) continue;
+            }
+            if (!boxes_overlap(box, bounds + 6 * std::uint64_t(j))) continue;
+            const uint2 pair = id < other ? make_uint2(f, j) : make_uint2(j, f);
+            const std::uint32_t at_kept = lower_bound_pair(kept, kept_count, g.ids, pair);
+            if (at_kept < kept_count && kept[at_kept].x == pair.x && kept[at_kept].y == pair.y) continue;
+            if (pairs != nullptr) pairs[base + found] = pair;
+            ++found;
+          }
+        }
+      }
+    }
+    if (pairs == nullptr) counts[i] = found;
+  }
+}
+
+// The fast pairs in (first id, second id) order: each pair's place is the
+// number of pairs before it (all pairs are distinct).
+__global__ void sort_fast_pairs_kernel(const uint2* __restrict__ in, std::uint32_t m, const std::uint64_t* __restrict__ ids,
+                                       uint2* __restrict__ out) {
+  for (std::uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < m; p += gridDim.x * blockDim.x) {
+    const uint2 mine = in[p];
+    std::uint32_t place = 0;
+    for (std::uint32_t q = 0; q < m; ++q) place += pair_before(ids, in[q], mine) ? 1u : 0u;
+    out[place] = mine;
+  }
+}
+
+// Each sorted new pair j at its place in the merged list, j + (kept pairs
+// before it), found by bisection of the kept list; shift[kept pairs before
+// it] counts it for the kept pairs' places.
+__global__ void place_fast_pairs_kernel(const uint2* __restrict__ sorted_fast, std::uint32_t m,
+                                        const uint2* __restrict__ kept, std::uint32_t kept_count,
+                                        const std::uint64_t* __restrict__ ids, uint2* __restrict__ merged,
+                                        std::uint32_t* __restrict__ shift) {
+  for (std::uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const uint2 p = sorted_fast[j];
+    const std::uint32_t before = lower_bound_pair(kept, kept_count, ids, p);
+    merged[j + before] = p;
+    atomicAdd(&shift[before], 1u);
+  }
+}
+
+// Each kept pair k at its place: k plus the new pairs before it
+// (shift_scan[k + 1], an exclusive scan of shift).
+__global__ void place_kept_pairs_kernel(const uint2* __restrict__ kept, std::uint32_t kept_count,
+                                        const std::uint32_t* __restrict__ shift_scan, uint2* __restrict__ merged) {
+  for (std::uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < kept_count; k += gridDim.x * blockDim.x) {
+    merged[k + shift_scan[k + 1]] = kept[k];
+  }
+}
+
 // ---------------------------------------------------------- narrow phase
 
 struct Capsule {
@@ -1083,6 +1251,47 @@ void launch_check_unique_ids(const std::uint64_t* ids, const std::uint32_t* orde
 void launch_max_u64(const std::uint64_t* values, std::uint32_t count, std::uint64_t* result, cudaStream_t stream) {
   max_u64_kernel<<<grid_for(count, kThreads), kThreads, 0, stream>>>(values, count,
                                                                       reinterpret_cast<unsigned long long*>(result));
+  count_launch();
+}
+
+
+void launch_fast_cells(GeometryView from, GeometryView to, double allowance, std::uint32_t* fast, std::uint32_t* list,
+                       std::uint32_t* count, cudaStream_t stream) {
+  if (to.count == 0) return;
+  fast_cells_kernel<<<grid_for(to.count, kThreads), kThreads, 0, stream>>>(from, to, allowance, fast, list, count);
+  count_launch();
+}
+
+void launch_fast_partners(GeometryView g, const double* bounds, const GridParams* grid,
+                          const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
+                          const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* fast,
+                          const std::uint32_t* list, const std::uint32_t* fast_count, std::uint32_t cap,
+                          const uint2* kept, std::uint32_t kept_count, std::uint32_t* counts,
+                          const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream) {
+  if (cap == 0) return;
+  fast_partners_kernel<<<grid_for(cap, 128, 16), 128, 0, stream>>>(g, bounds, grid, bucket_starts, sorted_lo, sorted_hi,
+                                                                   sorted_id, cell_coords, fast, list, fast_count, cap,
+                                                                   kept, kept_count, counts, offsets, pairs);
+  count_launch();
+}
+
+void launch_merge_fast_pairs(const uint2* fast_pairs, std::uint32_t fast_pair_count, uint2* sorted_fast,
+                             const uint2* kept, std::uint32_t kept_count, const std::uint64_t* ids,
+                             std::uint32_t* shift, std::uint32_t* shift_scan, std::uint32_t* temp, uint2* merged,
+                             cudaStream_t stream) {
+  // Every place of the merged list is written below; zeroed first so that
+  // no place can ever hold anything but a valid slot pair.
+  cudaMemsetAsync(merged, 0, (std::uint64_t(kept_count) + fast_pair_count) * sizeof(uint2), stream);
+  cudaMemsetAsync(shift, 0, (kept_count + 1ull) * sizeof(std::uint32_t), stream);
+  if (fast_pair_count > 0) {
+    sort_fast_pairs_kernel<<<grid_for(fast_pair_count, 128), 128, 0, stream>>>(fast_pairs, fast_pair_count, ids,
+                                                                             sorted_fast);
+    place_fast_pairs_kernel<<<grid_for(fast_pair_count, 128), 128, 0, stream>>>(sorted_fast, fast_pair_count, kept,
+                                                                              kept_count, ids, merged, shift);
+    count_launch(2);
+  }
+  exclusive_scan(shift, shift_scan, kept_count + 1ull, temp, stream);
+  place_kept_pairs_kernel<<<grid_for(kept_count, kThreads), kThreads, 0, stream>>>(kept, kept_count, shift_scan, merged);
   count_launch();
 }
 

@@ -168,6 +168,7 @@ enum Scalar : int {
   kInvalid = 3,
   kGrowthBits = 4,
   kDisplacementBits = 5,
+  kFastCount = 6,
   kScalarCount = 16
 };
 
@@ -492,6 +493,15 @@ struct msb_context {
   // re-checks of its refinement rounds reuse while the cells have moved less
   // than half of kept_margin (flag_overlaps).
   msb::DBuf<uint2> kept_pairs;
+  // Partial re-search (find_touches_partial): fast-cell flags and list, their
+  // new partners and the merge's shifts.
+  msb::DBuf<std::uint32_t> fast_flags, fast_list, fast_counts, fast_offsets, shift, shift_scan;
+  msb::DBuf<uint2> fast_pairs, fast_sorted;
+  // Overlap re-checks of the last step by kind: a full search, the kept
+  // candidates, the kept candidates with a partial re-search.  search_reuse:
+  // 0 all kinds, 1 no partial re-search, 2 full searches only.
+  std::uint32_t searches[3] = {0, 0, 0};
+  std::uint32_t search_reuse = 0;
   std::uint32_t kept_count = 0;
   float kept_margin = 0.0f;
   bool kept_valid = false;
@@ -921,27 +931,15 @@ std::uint32_t narrow_touches(Ctx& c, const GeometryView& g, ContactSearchParams 
   return touch_count;
 }
 
-// Cell-pair touches of `geometry` at prm.margin into out[0, count); returns
-// count.  The broad phase pads the boxes by `candidate_margin` >= prm.margin;
-// with a wider one the narrow phase first applies the box test at
-// prm.margin, so the touches are those of a search at prm.margin.  With
-// `keep` the candidate pairs stay in c.kept_pairs.
-std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DBuf<Touch>& out,
-                         float candidate_margin = -1.0f, bool keep = false) {
-  candidate_margin = std::max(candidate_margin, prm.margin);
+// The grid of `g` with boxes padded by `margin`: the cells' FP64 boxes, the
+// grid parameters, and the cells sorted by bucket with their FP32 boxes.
+void build_grid(Ctx& c, const GeometryView& g, float margin) {
   const std::uint32_t n = c.n;
-  if (keep) {
-    c.kept_valid = true;
-    c.kept_count = 0;
-    c.kept_margin = candidate_margin;
-  }
-  if (n < 2) return 0;
-  const GeometryView g = view_of(c, geometry);
   const std::uint32_t partials = bound_partials(n);
   c.bounds.ensure(6ull * n);
   c.bound_partials.ensure(10ull * partials);
   c.grid.ensure(1);
-  launch_cell_bounds(g, candidate_margin, c.bounds.p, c.bound_partials.p, c.stream);
+  launch_cell_bounds(g, margin, c.bounds.p, c.bound_partials.p, c.stream);
   const std::uint64_t capacity = grid_bucket_capacity(n);
   launch_grid_setup(c.bound_partials.p, partials, n, capacity, c.grid.p, c.stream, c.box_scale, c.colonies);
   c.cell_bucket.ensure(n);
@@ -959,6 +957,25 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   exclusive_scan(c.bucket_counts.p, c.bucket_starts.p, capacity, c.temp.p, c.stream);
   launch_scatter_cells(g, c.bounds.p, c.cell_bucket.p, c.bucket_starts.p, c.bucket_fill.p, c.sorted_lo.p, c.sorted_hi.p,
                        c.sorted_id.p, c.stream);
+}
+
+// Cell-pair touches of `geometry` at prm.margin into out[0, count); returns
+// count.  The broad phase pads the boxes by `candidate_margin` >= prm.margin;
+// with a wider one the narrow phase first applies the box test at
+// prm.margin, so the touches are those of a search at prm.margin.  With
+// `keep` the candidate pairs stay in c.kept_pairs.
+std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DBuf<Touch>& out,
+                         float candidate_margin = -1.0f, bool keep = false) {
+  candidate_margin = std::max(candidate_margin, prm.margin);
+  const std::uint32_t n = c.n;
+  if (keep) {
+    c.kept_valid = true;
+    c.kept_count = 0;
+    c.kept_margin = candidate_margin;
+  }
+  if (n < 2) return 0;
+  const GeometryView g = view_of(c, geometry);
+  build_grid(c, g, candidate_margin);
   c.cand_counts.ensure(n + 1ull);
   c.cand_offsets.ensure(n + 1ull);
   c.slab.ensure(std::size_t(n) * kSlabPartners);
@@ -1046,6 +1063,76 @@ std::uint32_t find_touches_kept(Ctx& c, Geometry& geometry, const msb_contact_pa
   const std::uint32_t pairs = narrow_touches(c, view_of(c, geometry), prm, c.kept_pairs.p, c.kept_count, out);
   const std::uint32_t walls = find_walls(c, geometry, 0.0f, wp.degeneracy_epsilon, true, out, pairs);
   return pairs + walls;
+}
+
+// Fast cells at most, and new pairs at most, for a partial re-search;
+// beyond either the re-check runs a full search.
+constexpr std::uint32_t kPartialPairs = 8192;
+std::uint32_t partial_cells(std::uint32_t n) { return std::max<std::uint32_t>(64, n / 64); }
+
+// The touches of find_touches at margin 0 on `geometry` when some cells
+// moved further than the kept candidates allow.  The kept pairs of two cells
+// that did not are still every such pair of the search (by the argument of
+// find_touches_kept); the pairs of the others are searched again on a grid
+// of `geometry`, and those the kept list lacks (usually none) are merged in,
+// in (first id, second id) order; then the constraint faces.  The same
+// touches in the same order as a full search.  Returns false, and no
+// touches, when more cells or pairs moved than the partial search takes.
+bool find_touches_partial(Ctx& c, Geometry& geometry, const msb_contact_parameters& cp,
+                          const msb_constraint_contact_parameters& wp, DBuf<Touch>& out, std::uint32_t& count) {
+  const std::uint32_t n = c.n;
+  if (!c.kept_valid || n < 2) return false;
+  const GeometryView from = view_of(c, c.base);
+  const GeometryView g = view_of(c, geometry);
+  const std::uint32_t cap = partial_cells(n);
+  const std::uint32_t kept = c.kept_count;
+  c.fast_flags.ensure(n);
+  c.fast_list.ensure(n);
+  check(cudaMemsetAsync(c.scalars.p + kFastCount, 0, 4, c.stream), "memset");
+  launch_fast_cells(from, g, double(c.kept_margin) - 1.0e-6, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount,
+                    c.stream);
+  build_grid(c, g, 0.0f);
+  c.fast_counts.ensure(cap + 1ull);
+  c.fast_offsets.ensure(cap + 1ull);
+  c.temp.ensure(scan_temp_words(std::max<std::uint64_t>(cap, kept) + 1ull) + 64);
+  check(cudaMemsetAsync(c.fast_counts.p + cap, 0, 4, c.stream), "memset");
+  launch_fast_partners(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
+                       c.coords.p, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount, cap, c.kept_pairs.p, kept,
+                       c.fast_counts.p, nullptr, nullptr, c.stream);
+  exclusive_scan(c.fast_counts.p, c.fast_offsets.p, cap + 1ull, c.temp.p, c.stream);
+  // The fast cells' number, the new pairs' number and the grid's status in one round trip.
+  GridParams grid{};
+  check(cudaMemcpyAsync(&c.host_scalars[kScalarCount + 5], c.fast_offsets.p + cap, 4, cudaMemcpyDeviceToHost,
+                        c.stream),
+        "read");
+  check(cudaMemcpyAsync(&grid, c.grid.p, sizeof(GridParams), cudaMemcpyDeviceToHost, c.stream), "read grid");
+  read_scalars(c);
+  if (grid.status == 1) throw std::invalid_argument("cell geometry is not finite");
+  if (grid.status != 0) throw DeviceCheckError("grid bucket capacity exceeded");
+  const std::uint32_t fast_count = c.host_scalars[kFastCount];
+  const std::uint32_t added = c.host_scalars[kScalarCount + 5];
+  if (fast_count > cap || added > kPartialPairs) return false;
+  ContactSearchParams prm{0.0f, cp.parallel_sine_threshold, cp.degeneracy_epsilon};
+  prm.box_margin = 0.0f;
+  std::uint32_t pairs = 0;
+  if (added == 0) {
+    pairs = narrow_touches(c, g, prm, c.kept_pairs.p, kept, out);
+  } else {
+    c.fast_pairs.ensure(added + 1ull);
+    c.fast_sorted.ensure(added + 1ull);
+    launch_fast_partners(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
+                         c.coords.p, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount, cap, c.kept_pairs.p,
+                         kept, nullptr, c.fast_offsets.p, c.fast_pairs.p, c.stream);
+    c.shift.ensure(kept + 1ull);
+    c.shift_scan.ensure(kept + 1ull);
+    c.pairs.ensure(std::size_t(kept) + added + 1);
+    launch_merge_fast_pairs(c.fast_pairs.p, added, c.fast_sorted.p, c.kept_pairs.p, kept, c.ids.p, c.shift.p,
+                            c.shift_scan.p, c.temp.p, c.pairs.p, c.stream);
+    pairs = narrow_touches(c, g, prm, c.pairs.p, kept + added, out);
+  }
+  const std::uint32_t walls = find_walls(c, geometry, 0.0f, wp.degeneracy_epsilon, true, out, pairs);
+  count = pairs + walls;
+  return true;
 }
 
 // Whether the last move allows find_touches_kept.
@@ -1353,8 +1440,15 @@ Overlaps flag_overlaps(Ctx& c, const msb_contact_parameters& cp, const msb_const
                        const msb_contact_dynamics_parameters& p) {
   Overlaps o;
   mark(c, kPhaseSearch);
-  o.candidates = kept_candidates_hold(c) ? find_touches_kept(c, c.state, cp, wp, c.found)
-                                         : find_touches(c, c.state, cp, wp, 0.0f, c.found);
+  if (c.search_reuse < 2 && kept_candidates_hold(c)) {
+    o.candidates = find_touches_kept(c, c.state, cp, wp, c.found);
+    ++c.searches[1];
+  } else if (c.search_reuse < 1 && find_touches_partial(c, c.state, cp, wp, c.found, o.candidates)) {
+    ++c.searches[2];
+  } else {
+    o.candidates = find_touches(c, c.state, cp, wp, 0.0f, c.found);
+    ++c.searches[0];
+  }
   mark(c, kPhaseMove);
   c.flags.ensure(o.candidates + 1ull);
   c.flag_offsets.ensure(o.candidates + 1ull);
@@ -1985,6 +2079,20 @@ int msb_last_step_solves(const msb_context* context, msb_solve_record* records, 
   return log.size() > capacity ? MSB_ERR_CAPACITY : MSB_OK;
 }
 
+int msb_last_step_searches(const msb_context* context, uint32_t* full, uint32_t* kept, uint32_t* partial) {
+  if (context == nullptr || full == nullptr || kept == nullptr || partial == nullptr) return MSB_ERR_INVALID_ARGUMENT;
+  *full = context->searches[0];
+  *kept = context->searches[1];
+  *partial = context->searches[2];
+  return MSB_OK;
+}
+
+int msb_set_search_reuse(msb_context* context, uint32_t mode) {
+  if (context == nullptr || mode > 2) return MSB_ERR_INVALID_ARGUMENT;
+  context->search_reuse = mode;
+  return MSB_OK;
+}
+
 int msb_set_flow_field(msb_context* context, const msb_flow_field* field) {
   if (context == nullptr) return MSB_ERR_INVALID_ARGUMENT;
   auto& c = *context;
@@ -2512,6 +2620,7 @@ static int advance_entry(msb_context* context, msb_cell_arrays* cells, const msb
     auto& c = *context;
     c.phase_marks.clear();
     c.solve_log.clear();
+    std::fill(std::begin(c.searches), std::end(c.searches), 0u);
     mark(c, kPhaseLoad);
     load_cells(c, *cells, device_pointers);
     load_constraints(c, constraints, constraint_count);
@@ -2617,6 +2726,7 @@ int msb_advance_contact_dynamics_batch(msb_context* context, msb_cell_arrays* ce
     c.box_scale = c.batch_box_scale;
     c.phase_marks.clear();
     c.solve_log.clear();
+    std::fill(std::begin(c.searches), std::end(c.searches), 0u);
     mark(c, kPhaseLoad);
     load_cells(c, *cells, device_pointers != 0);
     c.constraint_count = 0;

@@ -142,6 +142,25 @@ constexpr std::uint32_t kSlabPartners = 32;
 // the pair list (counts and offsets by id rank; order: slots by id rank).
 void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std::uint32_t* offsets,
                          const std::uint32_t* order, const std::uint32_t* slab, uint2* pairs, cudaStream_t stream);
+// Partial re-search of an overlap re-check (contacts.cu): the cells that
+// moved further than the kept candidates allow (`allowance` = the kept
+// padding margin less 1e-6: fast when 2 * moved > allowance), listed in
+// `list` with *count (zeroed by the caller); the fast cells' partners on the
+// current geometry's grid that the kept list lacks (count pass with pairs
+// null, over `cap` list places, then fill); and the kept list merged with
+// them in (first id, second id) order into `merged`.
+void launch_fast_cells(GeometryView from, GeometryView to, double allowance, std::uint32_t* fast, std::uint32_t* list,
+                       std::uint32_t* count, cudaStream_t stream);
+void launch_fast_partners(GeometryView g, const double* bounds, const GridParams* grid,
+                          const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
+                          const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* fast,
+                          const std::uint32_t* list, const std::uint32_t* fast_count, std::uint32_t cap,
+                          const uint2* kept, std::uint32_t kept_count, std::uint32_t* counts,
+                          const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream);
+void launch_merge_fast_pairs(const uint2* fast_pairs, std::uint32_t fast_pair_count, uint2* sorted_fast,
+                             const uint2* kept, std::uint32_t kept_count, const std::uint64_t* ids,
+                             std::uint32_t* shift, std::uint32_t* shift_scan, std::uint32_t* temp, uint2* merged,
+                             cudaStream_t stream);
 // Narrow phase: per candidate, the number of contacts below the margin
 // (count pass, `touches` null) or the contacts themselves at offsets[pair].
 void launch_narrow_phase(GeometryView g, const uint2* pairs, std::uint64_t pair_count,
