@@ -58,9 +58,11 @@ def test_partial_re_search_steps_as_full_searches():
 
 
 def test_partial_re_search_in_a_batch_steps_as_full_searches():
-    """Sixteen sweep colonies from their loose random starts, stepped as one
-    batch: every kind of re-check against full searches only."""
-    batch = sweep.sweep_batch(count=16, low=500, high=20_000, seed=3)
+    """Thirty-two sweep colonies of 5,000-40,000 capsules (above the size
+    from which a batch takes partial re-searches) from their loose random
+    starts, stepped as one batch: every kind of re-check against full
+    searches only."""
+    batch = sweep.sweep_batch(count=32, low=5_000, high=40_000, seed=3)
     auto, full = B200Backend(0), B200Backend(0)
     try:
         full.set_search_reuse(2)
