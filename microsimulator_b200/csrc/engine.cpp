@@ -206,6 +206,8 @@ constexpr float kRecheckReach = 0.15f;
 // area fraction 0.7, colonies growing from loose starts) measured 61-62 ms
 // per step at 0.15 um, 50-51 ms at 0.4 um and 52-53 ms at 1.0 um.
 constexpr float kBatchRecheckReach = 0.4f;
+// Active colonies at most for the batched solve's wide clusters (solve_batch).
+constexpr std::uint32_t kFewColonies = 96;
 constexpr float kMaximumSubstepRotation = 0.5f;
 constexpr float kPlannedSubstepRotation = 0.8f * kMaximumSubstepRotation;
 
@@ -564,6 +566,7 @@ struct msb_context {
   msb::BatchShape batch_shape{4, 256, false};
   int batch_clusters = 0;
   bool batch_tuned = false;
+  std::vector<std::uint32_t> host_colony_active;
   float box_scale = 1.0f;        // the contact search's box scale for the current call
   float batch_box_scale = 1.0f;  // the autotuner's choice for batches
   bool tune_search = true;
@@ -1393,7 +1396,25 @@ SolveOutcome solve_batch(Ctx& c, float dt, const msb_growth_load_response& growt
                                  c.stream);
   const msb::BatchDesc d = batch_desc(c, dt, growth, max_iterations);
   if (!c.batch_tuned) tune_batch(c, d);
-  run_batch(c, d, c.batch_shape, c.batch_clusters);
+  // A solve of few colonies (a step's later refinement rounds, where most
+  // colonies have settled) runs them on clusters of 16 CTAs: the largest
+  // colonies then set the time, and twice the CTAs halve their iteration
+  // (256-colony sweep, 3.0M capsules: 100k-row colonies 131 -> 63 us an
+  // iteration; solves of 3 colonies 1.8-2.0 -> 1.1 ms, of 83 5.0 -> 4.8 ms).
+  // With many colonies the tuned shape's more clusters serve them better.
+  c.host_colony_active.resize(k);
+  check(cudaMemcpyAsync(c.host_colony_active.data(), c.colony_active.p, k * 4ull, cudaMemcpyDeviceToHost, c.stream),
+        "read active colonies");
+  sync(c);
+  std::uint32_t active = 0;
+  for (const std::uint32_t a : c.host_colony_active) active += a != 0u ? 1u : 0u;
+  const msb::BatchShape wide{16, 512, true};
+  const int wide_clusters = active > 0 && active <= kFewColonies ? batch_resident_clusters(wide) : 0;
+  if (wide_clusters > 0) {
+    run_batch(c, d, wide, std::min<int>(wide_clusters, int(active)));
+  } else {
+    run_batch(c, d, c.batch_shape, c.batch_clusters);
+  }
   c.host_colony_state.resize(k);
   check(cudaMemcpyAsync(c.host_colony_state.data(), c.colony_state.p, k * sizeof(msb::ColonyState),
                         cudaMemcpyDeviceToHost, c.stream),
