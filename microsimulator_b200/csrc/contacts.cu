@@ -439,16 +439,20 @@ __device__ __forceinline__ std::uint32_t lower_bound_pair(const uint2* sorted, s
 // The partners of each listed fast cell on the grid of the current
 // geometry (boxes at margin 0): every cell whose FP64 box overlaps its own,
 // except another fast cell of lower id (whose own query lists that pair) and
-// the pairs the kept list holds.  Count pass (pairs null): counts[i]; fill
-// pass: the pairs at offsets[i], each as (lower-id slot, higher-id slot).
-// The listed cells' number is read from *fast_count.
+// the pairs the kept list holds (a cell's kept pairs as first cell are
+// kept[kept_offsets[rank[cell]] ...], the broad phase's list order).  Count
+// pass (pairs null): counts[i]; fill pass: the pairs at offsets[i], each as
+// (lower-id slot, higher-id slot).  The listed cells' number is read from
+// *fast_count.
 __global__ void fast_partners_kernel(GeometryView g, const double* __restrict__ bounds, const GridParams* grid_ptr,
                                      const std::uint32_t* __restrict__ starts, const float4* __restrict__ sorted_lo,
                                      const float4* __restrict__ sorted_hi, const std::uint64_t* __restrict__ sorted_id,
                                      const std::int64_t* __restrict__ coords, const std::uint32_t* __restrict__ fast,
                                      const std::uint32_t* __restrict__ list, const std::uint32_t* fast_count_ptr,
-                                     std::uint32_t cap, const uint2* __restrict__ kept, std::uint32_t kept_count,
-                                     std::uint32_t* __restrict__ counts, const std::uint32_t* __restrict__ offsets,
+                                     std::uint32_t cap, const uint2* __restrict__ kept,
+                                     const std::uint32_t* __restrict__ kept_offsets,
+                                     const std::uint32_t* __restrict__ rank, std::uint32_t* __restrict__ counts,
+                                     const std::uint32_t* __restrict__ offsets,
                                      uint2* __restrict__ pairs) {
   const GridParams grid = *grid_ptr;
   const std::uint32_t fast_count = *fast_count_ptr < cap ? *fast_count_ptr : cap;
@@ -502,8 +506,10 @@ __global__ void fast_partners_kernel(GeometryView g, const double* __restrict__ 
             }
             if (!boxes_overlap(box, bounds + 6 * std::uint64_t(j))) continue;
             const uint2 pair = id < other ? make_uint2(f, j) : make_uint2(j, f);
-            const std::uint32_t at_kept = lower_bound_pair(kept, kept_count, g.ids, pair);
-            if (at_kept < kept_count && kept[at_kept].x == pair.x && kept[at_kept].y == pair.y) continue;
+            const std::uint32_t r = rank[pair.x];
+            bool held = false;
+            for (std::uint32_t k = kept_offsets[r]; k < kept_offsets[r + 1] && !held; ++k) held = kept[k].y == pair.y;
+            if (held) continue;
             if (pairs != nullptr) pairs[base + found] = pair;
             ++found;
           }
@@ -1266,12 +1272,12 @@ void launch_fast_partners(GeometryView g, const double* bounds, const GridParams
                           const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
                           const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* fast,
                           const std::uint32_t* list, const std::uint32_t* fast_count, std::uint32_t cap,
-                          const uint2* kept, std::uint32_t kept_count, std::uint32_t* counts,
-                          const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream) {
+                          const uint2* kept, const std::uint32_t* kept_offsets, const std::uint32_t* rank,
+                          std::uint32_t* counts, const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream) {
   if (cap == 0) return;
   fast_partners_kernel<<<grid_for(cap, 128, 16), 128, 0, stream>>>(g, bounds, grid, bucket_starts, sorted_lo, sorted_hi,
                                                                    sorted_id, cell_coords, fast, list, fast_count, cap,
-                                                                   kept, kept_count, counts, offsets, pairs);
+                                                                   kept, kept_offsets, rank, counts, offsets, pairs);
   count_launch();
 }
 

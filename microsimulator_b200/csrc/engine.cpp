@@ -495,6 +495,7 @@ struct msb_context {
   // re-checks of its refinement rounds reuse while the cells have moved less
   // than half of kept_margin (flag_overlaps).
   msb::DBuf<uint2> kept_pairs;
+  msb::DBuf<std::uint32_t> kept_offsets;
   // Partial re-search (find_touches_partial): fast-cell flags and list, their
   // new partners and the merge's shifts.
   msb::DBuf<std::uint32_t> fast_flags, fast_list, fast_counts, fast_offsets, shift, shift_scan;
@@ -1014,6 +1015,7 @@ std::uint32_t find_pairs(Ctx& c, Geometry& geometry, ContactSearchParams prm, DB
   const std::uint32_t touch_count = narrow_touches(c, g, prm, c.pairs.p, pair_count, out);
   if (keep) {
     std::swap(c.pairs, c.kept_pairs);
+    std::swap(c.cand_offsets, c.kept_offsets);  // the kept pairs by first cell's rank
     c.kept_count = pair_count;
   }
   return touch_count;
@@ -1072,10 +1074,13 @@ std::uint32_t find_touches_kept(Ctx& c, Geometry& geometry, const msb_contact_pa
 // beyond either the re-check runs a full search.  Below kPartialFromCells
 // cells a full search costs less than the partial one's fixed part (the grid
 // of the current geometry and the fast cells' queries): at 100k capsules of
-// the trap colony 285 us against 320-730 us.
+// the trap colony 285 us against 320-730 us.  Each fast cell's query is one
+// thread's walk of its neighbour boxes, so thousands of them cost more than
+// the broad phase of every cell (1M capsules: up to 16k fast cells took
+// 1.2 ms a query launch against 0.7 ms for the broad phase): at most 1,024.
 constexpr std::uint32_t kPartialPairs = 8192;
 constexpr std::uint32_t kPartialFromCells = 262144;
-std::uint32_t partial_cells(std::uint32_t n) { return std::max<std::uint32_t>(64, n / 64); }
+std::uint32_t partial_cells(std::uint32_t n) { return std::clamp<std::uint32_t>(n / 1024, 64, 1024); }
 
 // The touches of find_touches at margin 0 on `geometry` when some cells
 // moved further than the kept candidates allow.  The kept pairs of two cells
@@ -1093,6 +1098,7 @@ bool find_touches_partial(Ctx& c, Geometry& geometry, const msb_contact_paramete
   const GeometryView g = view_of(c, geometry);
   const std::uint32_t cap = partial_cells(n);
   const std::uint32_t kept = c.kept_count;
+  if (kept == 0) return false;  // no kept list (nor its offsets) to search beside
   c.fast_flags.ensure(n);
   c.fast_list.ensure(n);
   check(cudaMemsetAsync(c.scalars.p + kFastCount, 0, 4, c.stream), "memset");
@@ -1104,8 +1110,8 @@ bool find_touches_partial(Ctx& c, Geometry& geometry, const msb_contact_paramete
   c.temp.ensure(scan_temp_words(std::max<std::uint64_t>(cap, kept) + 1ull) + 64);
   check(cudaMemsetAsync(c.fast_counts.p + cap, 0, 4, c.stream), "memset");
   launch_fast_partners(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
-                       c.coords.p, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount, cap, c.kept_pairs.p, kept,
-                       c.fast_counts.p, nullptr, nullptr, c.stream);
+                       c.coords.p, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount, cap, c.kept_pairs.p,
+                       c.kept_offsets.p, c.rank.p, c.fast_counts.p, nullptr, nullptr, c.stream);
   exclusive_scan(c.fast_counts.p, c.fast_offsets.p, cap + 1ull, c.temp.p, c.stream);
   // The fast cells' number, the new pairs' number and the grid's status in one round trip.
   GridParams grid{};
@@ -1129,7 +1135,7 @@ bool find_touches_partial(Ctx& c, Geometry& geometry, const msb_contact_paramete
     c.fast_sorted.ensure(added + 1ull);
     launch_fast_partners(g, c.bounds.p, c.grid.p, c.bucket_starts.p, c.sorted_lo.p, c.sorted_hi.p, c.sorted_id.p,
                          c.coords.p, c.fast_flags.p, c.fast_list.p, c.scalars.p + kFastCount, cap, c.kept_pairs.p,
-                         kept, nullptr, c.fast_offsets.p, c.fast_pairs.p, c.stream);
+                         c.kept_offsets.p, c.rank.p, nullptr, c.fast_offsets.p, c.fast_pairs.p, c.stream);
     c.shift.ensure(kept + 1ull);
     c.shift_scan.ensure(kept + 1ull);
     c.pairs.ensure(std::size_t(kept) + added + 1);

@@ -146,8 +146,9 @@ void launch_compact_slab(std::uint32_t n, const std::uint32_t* counts, const std
 // moved further than the kept candidates allow (`allowance` = the kept
 // padding margin less 1e-6: fast when 2 * moved > allowance), listed in
 // `list` with *count (zeroed by the caller); the fast cells' partners on the
-// current geometry's grid that the kept list lacks (count pass with pairs
-// null, over `cap` list places, then fill); and the kept list merged with
+// current geometry's grid that the kept list lacks (its pairs by first cell
+// at kept_offsets[rank[cell]]; count pass with pairs null, over `cap` list
+// places, then fill); and the kept list merged with
 // them in (first id, second id) order into `merged`.
 void launch_fast_cells(GeometryView from, GeometryView to, double allowance, std::uint32_t* fast, std::uint32_t* list,
                        std::uint32_t* count, cudaStream_t stream);
@@ -155,8 +156,8 @@ void launch_fast_partners(GeometryView g, const double* bounds, const GridParams
                           const std::uint32_t* bucket_starts, const float4* sorted_lo, const float4* sorted_hi,
                           const std::uint64_t* sorted_id, const std::int64_t* cell_coords, const std::uint32_t* fast,
                           const std::uint32_t* list, const std::uint32_t* fast_count, std::uint32_t cap,
-                          const uint2* kept, std::uint32_t kept_count, std::uint32_t* counts,
-                          const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream);
+                          const uint2* kept, const std::uint32_t* kept_offsets, const std::uint32_t* rank,
+                          std::uint32_t* counts, const std::uint32_t* offsets, uint2* pairs, cudaStream_t stream);
 void launch_merge_fast_pairs(const uint2* fast_pairs, std::uint32_t fast_pair_count, uint2* sorted_fast,
                              const uint2* kept, std::uint32_t kept_count, const std::uint64_t* ids,
                              std::uint32_t* shift, std::uint32_t* shift_scan, std::uint32_t* temp, uint2* merged,
