@@ -633,6 +633,7 @@ def main():
     # solve (rows * 96 + cells * 128 per iteration) and the solve phase's
     # CUDA-event time on the backend's stream.
     live = {"bytes": 0, "iterations": 0, "solve_ms": 0.0}
+    rechecks = {"full": 0, "kept": 0, "partial": 0}
 
     def timed(world, mode, record=False):
         """K steps from `world`; device time, cell-steps, iterations and
@@ -650,13 +651,17 @@ def main():
                 phases[name] += value / args.steps
             per_step.append({"cells": len(world), "ms": round(ms, 3), "iterations": int(report.iterations),
                              "load_ms": round(step_phases["load"], 3), "solve_ms": round(step_phases["solve"], 3)})
-        if record and rank == 0:
-            print(json.dumps({"arm": "timed_steps", "mode": mode, "steps": per_step}), file=sys.stderr)
             if record:
+                # Every timed step's solves: bytes and iterations, and the
+                # solve phase's device time.
                 for solve in backend.last_step_solves():
                     live["bytes"] += (int(solve["rows"]) * 96 + len(world) * 128) * int(solve["iterations"])
                     live["iterations"] += int(solve["iterations"])
                 live["solve_ms"] += step_phases["solve"]
+                for name, count in backend.last_step_searches().items():
+                    rechecks[name] += count
+        if record and rank == 0:
+            print(json.dumps({"arm": "timed_steps", "mode": mode, "steps": per_step}), file=sys.stderr)
         return total_ms, cell_steps, iterations, phases
 
     for step in range(args.warmup):
@@ -795,6 +800,8 @@ def main():
             "contact_graph": graph_line,
             "walls": walls_line,
             "phase_ms_per_step": phases,
+            # The timed steps' overlap re-checks by how their candidates were found.
+            "rechecks": rechecks,
             "roofline": {
                 "kernel": "bb_iteration (body pass + row pass)",
                 "bound": "hbm",
