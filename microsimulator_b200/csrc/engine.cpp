@@ -2119,9 +2119,10 @@ int msb_last_step_searches(const msb_context* context, uint32_t* full, uint32_t*
 }
 
 int msb_set_search_reuse(msb_context* context, uint32_t mode) {
-  if (context == nullptr || mode > 2) return MSB_ERR_INVALID_ARGUMENT;
-  context->search_reuse = mode;
-  return MSB_OK;
+  return guarded(context, [&] {
+    if (mode > 2) throw std::invalid_argument("search reuse must be 0 (all kinds), 1 (no partial re-search) or 2 (full searches)");
+    context->search_reuse = mode;
+  });
 }
 
 int msb_set_flow_field(msb_context* context, const msb_flow_field* field) {

@@ -88,11 +88,9 @@ def test_partial_re_search_in_a_batch_steps_as_full_searches():
 
 
 def test_search_reuse_modes_are_checked(backend):
-    from microsimulator_b200 import abi
-
     for mode in (0, 1, 2):
         backend.set_search_reuse(mode)
-    with pytest.raises(abi.NativeError):
+    with pytest.raises(ValueError, match="search reuse"):
         backend.set_search_reuse(3)
     backend.set_search_reuse(0)
     assert set(backend.last_step_searches()) == {"full", "kept", "partial"}
